@@ -1,0 +1,245 @@
+/*
+ * mpulse_b200.h - C ABI of the B200 time-stepping path of MPulse.
+ *
+ * One context (mp_ctx) owns the device state of one simulation: the six Yee
+ * field components, the PLRC accumulators of the Lorentz poles, the CPML psi
+ * layers and the per-step injection planes.  The host calls mp_step() once per
+ * MPulse time step (or once for many steps); everything in between stays in HBM.
+ *
+ * What each entry point replaces in MPulse (paths relative to the MPulse tree):
+ *
+ *   mp_create      FieldSimulation::init (src/fieldsim.cpp:31-107) as far as the
+ *                  solver is concerned: FDTD_PLRCSolver::initStorage
+ *                  (src/fdtd_plrc.t:18-76), FDTD_PLRCCore::coreInitStorage
+ *                  (src/fdtd_plrc.cpp:13-86), CPMLBorder[OneD]::initCurrents /
+ *                  initCoefficients (src/cpml_border.cpp:14-139, :158-243),
+ *                  CPMLBorderCurrent::makeCoeff (src/cpml_border.cpp:287-339),
+ *                  IncidentSource::initCurrents (src/incsource.cpp:16-77).
+ *   mp_step        FieldSolver::stepScheme (src/fieldsolver.h:218-219) as
+ *                  implemented by FDTD_PLRCSolver::stepScheme
+ *                  (src/fdtd_plrc.t:127-168), FDTD_Plain::stepScheme
+ *                  (src/fdtd_plain.cpp:31-35) and FDTD_Nonlinear::stepScheme
+ *                  (src/fdtd_nl.cpp:32-36), including the boundary exchange of
+ *                  Storage::applyBoundary (src/storage.cpp:194-204) done by
+ *                  SinglePeriodicBoundary / SingleXYPeriodicBoundary
+ *                  (src/periodic_bound.cpp:10-130), which becomes an index wrap.
+ *                  One call advances n_steps steps; Process::time
+ *                  (src/process.cpp:22) is kept in the context.
+ *   mp_upload /    direct access to the Storage grids by name
+ *   mp_download    (Storage::getGrid, src/storage.cpp:48-51), e.g. by the field
+ *                  initialisers (src/pulseinit.cpp:22-27) and the diagnostics
+ *                  (src/fielddiag.cpp:255-286).
+ *   mp_last_error  replaces std::cerr + exit(-1) (e.g. src/fdtd_plrc.t:20-24).
+ *
+ * Conventions
+ *   - Every function returns 0 (MP_OK) or a negative mp_status; none exits.
+ *     The message of the last failure is available from mp_last_error().
+ *   - Host buffers are caller-owned and always double precision; the device
+ *     form (FP32 or FP64) is chosen by mp_config.precision.
+ *   - Field layout on the host side ("plane layout"): nz+2 z-planes, index
+ *     k = 0 .. nz+1 exactly as MPulse's global z index (src/globals.cpp:74-75);
+ *     x and y hold the interior only (MPulse indices 1..n), x fastest:
+ *         h[((size_t)k * ny + (j - 1)) * nx + (i - 1)]   for MPulse cell (i, j, k)
+ *     MPulse's x/y ghost cells are periodic images in both boundaries it
+ *     supports on one process and are not stored.  In the z-periodic boundary
+ *     the planes 0 and nz+1 are images of nz and 1; they are ignored on upload
+ *     and filled on download.
+ *   - A context is used by one host thread at a time; all device work goes to
+ *     the context's stream (mp_set_stream), so calls are asynchronous except
+ *     mp_download, mp_sync and the status check at the end of mp_step.
+ */
+#ifndef MPULSE_B200_H
+#define MPULSE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MP_ABI_VERSION 1
+#define MP_MAX_POLES 3
+#define MP_MAX_SOURCES 4
+
+typedef enum mp_status {
+  MP_OK = 0,
+  MP_ERR_INVALID = -1,      /* bad argument or configuration */
+  MP_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  MP_ERR_NO_MEMORY = -3,    /* device allocation failed */
+  MP_ERR_NEWTON = -4,       /* Kerr Newton solve did not converge in a cell */
+  MP_ERR_NONFINITE = -5,    /* a field value became NaN or Inf */
+  MP_ERR_UNSUPPORTED = -6,  /* the configuration names a part that is not built */
+  MP_ERR_NAME = -7          /* unknown field name */
+} mp_status;
+
+typedef enum mp_precision { MP_FP64 = 0, MP_FP32 = 1 } mp_precision;
+
+/* The solvers MPulse registers in FieldSimulation::MakeParamMap
+ * (src/fieldsim.cpp:177-195). */
+typedef enum mp_solver_kind {
+  MP_SOLVER_PLAIN = 0,       /* "fdtd-plain"       src/fdtd_plain.cpp */
+  MP_SOLVER_NL = 1,          /* "fdtd-nl"          src/fdtd_nl.cpp */
+  MP_SOLVER_PLRC_LIN = 2,    /* "fdtd-plrc-lin"    src/fdtd_plrc.cpp:94-293 */
+  MP_SOLVER_PLRC_NONLIN = 3  /* "fdtd-plrc-nonlin" src/fdtd_plrc.cpp:304-459 */
+} mp_solver_kind;
+
+/* The single-process boundaries (src/fieldsim.cpp:198-204). */
+typedef enum mp_boundary_kind {
+  MP_BOUNDARY_PERIODIC = 0,     /* "single_periodic"    periodic_bound.cpp:10-71 */
+  MP_BOUNDARY_XY_PERIODIC = 1   /* "single_xy_periodic" periodic_bound.cpp:87-130 */
+} mp_boundary_kind;
+
+/* CPML plug-ins (src/fdtd_plrc.t:439-445). */
+typedef enum mp_cpml_kind {
+  MP_CPML_NONE = 0,
+  MP_CPML_ALL = 1,   /* "cpml_border":    all six faces, cpml_border.cpp:14-139 */
+  MP_CPML_Z = 2      /* "cpml_border_1d": z faces only, cpml_border.cpp:158-243 */
+} mp_cpml_kind;
+
+/* Incident-source plug-ins (src/fdtd_plrc.t:447-469). */
+typedef enum mp_source_kind {
+  MP_SOURCE_NONE = 0,
+  MP_SOURCE_PLANE_WAVE = 1,     /* "wave_inject"        sources.cpp:8-173 */
+  MP_SOURCE_PLANE_GAUSS = 2,    /* "plane_gauss_inject" sources.cpp:179-331 */
+  MP_SOURCE_SHORT_PULSE = 3,    /* "short_pulse_inject" shortpulseinject.cpp */
+  MP_SOURCE_FOCUSED_PULSE = 4   /* "focused_pulse_inject" (see mp_source) */
+} mp_source_kind;
+
+/* One Lorentz pole: MPulse's L<n>eps, L<n>delta, L<n>Om2
+ * (src/fdtd_plrc.t:419-429, src/fdtd_plrc.h:85-90). */
+typedef struct mp_lorentz_pole {
+  double eps;    /* Delta epsilon of the pole */
+  double delta;  /* damping delta (e-folding rate of chi(t)) */
+  double om2;    /* resonance omega^2; must be > delta^2 and != 0 */
+} mp_lorentz_pole;
+
+/* One incident-source plug-in.  Only the fields of its kind are read. */
+typedef struct mp_source {
+  int kind;          /* mp_source_kind */
+  int distance;      /* "d": TF/SF plane index, incsource.cpp:84 (default 15) */
+  /* wave_inject, plane_gauss_inject (sources.cpp:58-82, :225-241) */
+  double k[3];       /* kx ky kz */
+  double H[3];       /* Hx Hy Hz */
+  double H_bg[3];    /* Hx_bg.. (wave_inject only) */
+  double E_bg[3];    /* Ex_bg.. (wave_inject only) */
+  double ramp;       /* wave_inject ramp (default 0.5) */
+  double width;      /* plane_gauss_inject width (default 10) */
+  double offset;     /* plane_gauss_inject offset (default 40) */
+  double eps;        /* background permittivity of the source (default 1) */
+  /* short_pulse_inject / focused_pulse_inject (shortpulseinject.cpp:33-49) */
+  double length;     /* pulse duration parameter T */
+  double waist;      /* "width": beam waist w0 */
+  double om0;        /* carrier frequency (default 2 pi) */
+  double t_shift;    /* TShift */
+  double z_shift;    /* ZShift (focus offset from the grid centre) */
+  double phase;      /* Phase, in units of 2 pi */
+  double amp;        /* peak amplitude of Re Ex at the focus */
+} mp_source;
+
+typedef struct mp_config {
+  int abi_version;          /* must be MP_ABI_VERSION */
+  int nx, ny, nz;           /* grid-x, grid-y, grid-z (globals.cpp:53-55) */
+  double dx, dy, dz;        /* grid-dx, grid-dy, grid-dz */
+  double dt;                /* dt */
+  int precision;            /* mp_precision of the device state */
+  int solver;               /* mp_solver_kind */
+  int boundary;             /* mp_boundary_kind */
+
+  /* medium (fdtd_plrc.t:417-429, fdtd_plrc.cpp:461-465, fdtd_nl.cpp:146-153) */
+  double eps;               /* eps_infinity of the medium */
+  double chi;               /* Kerr chi (PLRC_NONLIN and NL) */
+  mp_lorentz_pole poles[MP_MAX_POLES];
+  /* The medium fills the z-planes medium_z0..medium_z1 (MPulse z index,
+   * inclusive); cells outside are a background of permittivity eps_bg without
+   * poles or Kerr term.  MPulse itself has a uniform medium: medium_z0 = 0,
+   * medium_z1 = nz + 1. */
+  int medium_z0, medium_z1;
+  double eps_bg;
+
+  /* CPML (cpml_border.cpp:142-151) */
+  int cpml;                 /* mp_cpml_kind */
+  int cpml_d;               /* d: layer thickness (default 8) */
+  double cpml_kappa_max;    /* kappaMax (default 15) */
+  double cpml_a_max;        /* aMax (default 0.25) */
+  double cpml_sigma_max;    /* sigmaMax (default 3) */
+
+  int n_sources;
+  mp_source sources[MP_MAX_SOURCES];
+
+  /* Kerr Newton solve: MPulse iterates until |E - E_old| <= 1e-9 with no cap
+   * (fdtd_plrc.cpp:409-414).  Here the loop is capped; a cell that does not
+   * converge makes mp_step return MP_ERR_NEWTON. */
+  int newton_max_iter;      /* default 64 */
+  double newton_tol;        /* default 1e-9 */
+
+  int device;               /* CUDA device ordinal */
+} mp_config;
+
+typedef struct mp_ctx mp_ctx;
+
+/* Fills *cfg with MPulse's parameter defaults (the ParameterValue defaults of
+ * the MakeParamMap functions cited above) and a 32^3 grid. */
+void mp_config_defaults(mp_config *cfg);
+
+/* Allocates and zero-initialises all device state of a simulation.
+ * MPulse: FDTD_PLRCSolver::initStorage and the plug-ins' initStorage. */
+int mp_create(const mp_config *cfg, mp_ctx **out);
+
+/* Releases everything mp_create allocated.  Accepts NULL. */
+void mp_destroy(mp_ctx *ctx);
+
+/* Runs all further device work of ctx on the given cudaStream_t (NULL: the
+ * context's own stream). */
+int mp_set_stream(mp_ctx *ctx, void *cuda_stream);
+
+/* Number of doubles of the host buffer for field `name`.  Names follow
+ * MPulse's Storage: "Ex" "Ey" "Ez" "Bx" "By" "Bz" (fdtd_plrc.cpp:17-23) and the
+ * PLRC accumulators "PsiR<n><c>" / "PsiI<n><c>" with n = 1..3, c = x, y, z
+ * (fdtd_plrc.cpp:35-57), all in the plane layout described above. */
+int mp_field_size(mp_ctx *ctx, const char *name, size_t *count);
+
+/* Copies a host field into the device state (converted to the device form). */
+int mp_upload(mp_ctx *ctx, const char *name, const double *host, size_t count);
+
+/* Copies a device field to the host.  Synchronises the context's stream. */
+int mp_download(mp_ctx *ctx, const char *name, double *host, size_t count);
+
+/* Advances the simulation by n_steps MPulse time steps, each the stepScheme
+ * order of fdtd_plrc.t:127-168: E-side currents (CPML psi_E, TF/SF J), the D
+ * update with PLRC / Kerr, the E boundary, H-side currents (CPML psi_H, TF/SF
+ * M), the B update, the B boundary.  Synchronises once at the end to read the
+ * device status word (Newton failures, non-finite values). */
+int mp_step(mp_ctx *ctx, int n_steps);
+
+/* Same as mp_step, without the synchronisation and status check; the status
+ * is accumulated and returned by the next mp_check_status(). */
+int mp_step_async(mp_ctx *ctx, int n_steps);
+int mp_check_status(mp_ctx *ctx);
+
+/* Process::time of the next step (src/process.cpp:22); starts at 0. */
+int mp_get_time(mp_ctx *ctx, long long *time);
+int mp_set_time(mp_ctx *ctx, long long time);
+
+/* Waits for all work queued on the context's stream. */
+int mp_sync(mp_ctx *ctx);
+
+/* Device pointer, element count and element size (4 or 8 bytes) of a field's
+ * device array, for zero-copy use by a caller that already lives on the GPU.
+ * The device array has the plane layout above. */
+int mp_device_field(mp_ctx *ctx, const char *name, void **dptr, size_t *count,
+                    int *elem_bytes);
+
+/* Number of CUDA kernel launches the context has issued so far. */
+long long mp_launch_count(mp_ctx *ctx);
+
+/* Copies the message of the last failure (or "") into buf. */
+int mp_last_error(mp_ctx *ctx, char *buf, size_t n);
+
+/* Message of the last mp_create failure (no context exists then). */
+const char *mp_create_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPULSE_B200_H */

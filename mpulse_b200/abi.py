@@ -1,0 +1,196 @@
+"""ctypes mirror of include/mpulse_b200.h (mp_config and friends).
+
+The layout here must match the C header field for field; a CPU test compares
+``ctypes.sizeof`` and the defaults with the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+MP_ABI_VERSION = 1
+MP_MAX_POLES = 3
+MP_MAX_SOURCES = 4
+
+# mp_status
+MP_OK = 0
+MP_ERR_INVALID = -1
+MP_ERR_CUDA = -2
+MP_ERR_NO_MEMORY = -3
+MP_ERR_NEWTON = -4
+MP_ERR_NONFINITE = -5
+MP_ERR_UNSUPPORTED = -6
+MP_ERR_NAME = -7
+
+STATUS_NAMES = {
+    MP_OK: "MP_OK",
+    MP_ERR_INVALID: "MP_ERR_INVALID",
+    MP_ERR_CUDA: "MP_ERR_CUDA",
+    MP_ERR_NO_MEMORY: "MP_ERR_NO_MEMORY",
+    MP_ERR_NEWTON: "MP_ERR_NEWTON",
+    MP_ERR_NONFINITE: "MP_ERR_NONFINITE",
+    MP_ERR_UNSUPPORTED: "MP_ERR_UNSUPPORTED",
+    MP_ERR_NAME: "MP_ERR_NAME",
+}
+
+MP_FP64, MP_FP32 = 0, 1
+MP_SOLVER_PLAIN, MP_SOLVER_NL, MP_SOLVER_PLRC_LIN, MP_SOLVER_PLRC_NONLIN = 0, 1, 2, 3
+MP_BOUNDARY_PERIODIC, MP_BOUNDARY_XY_PERIODIC = 0, 1
+MP_CPML_NONE, MP_CPML_ALL, MP_CPML_Z = 0, 1, 2
+(MP_SOURCE_NONE, MP_SOURCE_PLANE_WAVE, MP_SOURCE_PLANE_GAUSS,
+ MP_SOURCE_SHORT_PULSE, MP_SOURCE_FOCUSED_PULSE) = range(5)
+
+FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz")
+PSI_NAMES = tuple(f"Psi{ri}{n}{c}" for ri in "RI" for n in (1, 2, 3) for c in "xyz")
+
+
+class LorentzPole(C.Structure):
+    _fields_ = [("eps", C.c_double), ("delta", C.c_double), ("om2", C.c_double)]
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("distance", C.c_int),
+        ("k", C.c_double * 3),
+        ("H", C.c_double * 3),
+        ("H_bg", C.c_double * 3),
+        ("E_bg", C.c_double * 3),
+        ("ramp", C.c_double),
+        ("width", C.c_double),
+        ("offset", C.c_double),
+        ("eps", C.c_double),
+        ("length", C.c_double),
+        ("waist", C.c_double),
+        ("om0", C.c_double),
+        ("t_shift", C.c_double),
+        ("z_shift", C.c_double),
+        ("phase", C.c_double),
+        ("amp", C.c_double),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int),
+        ("nx", C.c_int),
+        ("ny", C.c_int),
+        ("nz", C.c_int),
+        ("dx", C.c_double),
+        ("dy", C.c_double),
+        ("dz", C.c_double),
+        ("dt", C.c_double),
+        ("precision", C.c_int),
+        ("solver", C.c_int),
+        ("boundary", C.c_int),
+        ("eps", C.c_double),
+        ("chi", C.c_double),
+        ("poles", LorentzPole * MP_MAX_POLES),
+        ("medium_z0", C.c_int),
+        ("medium_z1", C.c_int),
+        ("eps_bg", C.c_double),
+        ("cpml", C.c_int),
+        ("cpml_d", C.c_int),
+        ("cpml_kappa_max", C.c_double),
+        ("cpml_a_max", C.c_double),
+        ("cpml_sigma_max", C.c_double),
+        ("n_sources", C.c_int),
+        ("sources", Source * MP_MAX_SOURCES),
+        ("newton_max_iter", C.c_int),
+        ("newton_tol", C.c_double),
+        ("device", C.c_int),
+    ]
+
+    def field_count(self) -> int:
+        """Doubles in one host buffer of the plane layout: (nz+2) * ny * nx."""
+        return (self.nz + 2) * self.ny * self.nx
+
+    def field_shape(self):
+        return (self.nz + 2, self.ny, self.nx)
+
+
+def default_source(kind: int = MP_SOURCE_NONE) -> Source:
+    """Parameter defaults of the injector plug-ins (incsource.cpp:84,
+    sources.cpp:62-79 and :229-239, shortpulseinject.cpp:38-46)."""
+    s = Source()
+    s.kind = kind
+    s.distance = 15
+    s.k[:] = (0.0, 0.0, 1.0)
+    s.H[:] = (0.0, 0.0, 0.0)
+    s.ramp = 0.5
+    s.width = 10.0
+    s.offset = 40.0
+    s.eps = 1.0
+    s.length = 1.0
+    s.waist = 1.0
+    s.om0 = 2 * math.pi
+    s.amp = 1.0
+    return s
+
+
+def default_config() -> Config:
+    """MPulse's ParameterValue defaults (globals.cpp:53-63 for dx/dt,
+    fdtd_plrc.t:417-429, fdtd_plrc.cpp:463, cpml_border.cpp:146-149) on a 32^3
+    grid; the same values as mp_config_defaults() in the C library."""
+    c = Config()
+    c.abi_version = MP_ABI_VERSION
+    c.nx = c.ny = c.nz = 32
+    c.dx = c.dy = c.dz = 0.1
+    c.dt = 1e-2
+    c.precision = MP_FP64
+    c.solver = MP_SOLVER_PLRC_LIN
+    c.boundary = MP_BOUNDARY_PERIODIC
+    c.eps = 1.0
+    c.chi = 0.1
+    for n in range(MP_MAX_POLES):
+        c.poles[n].eps = 0.0
+        c.poles[n].delta = 0.0
+        c.poles[n].om2 = 1.0
+    c.medium_z0 = 0
+    c.medium_z1 = 1 << 30
+    c.eps_bg = 1.0
+    c.cpml = MP_CPML_NONE
+    c.cpml_d = 8
+    c.cpml_kappa_max = 15.0
+    c.cpml_a_max = 0.25
+    c.cpml_sigma_max = 3.0
+    c.n_sources = 0
+    for n in range(MP_MAX_SOURCES):
+        c.sources[n] = default_source()
+    c.newton_max_iter = 64
+    c.newton_tol = 1e-9
+    c.device = 0
+    return c
+
+
+def config_to_dict(c: Config) -> dict:
+    """Plain-dict view of a Config (for logs and fixtures)."""
+    def conv(v):
+        if isinstance(v, C.Structure):
+            return {f: conv(getattr(v, f)) for f, _ in v._fields_}
+        if isinstance(v, C.Array):
+            return [conv(x) for x in v]
+        return v
+    return conv(c)
+
+
+def config_from_dict(d: dict) -> Config:
+    c = default_config()
+
+    def fill(obj, dd):
+        for f, _ in obj._fields_:
+            if f not in dd:
+                continue
+            v = getattr(obj, f)
+            if isinstance(v, C.Structure):
+                fill(v, dd[f])
+            elif isinstance(v, C.Array):
+                for n, x in enumerate(dd[f]):
+                    if isinstance(v[n], C.Structure):
+                        fill(v[n], x)
+                    else:
+                        v[n] = x
+            else:
+                setattr(obj, f, dd[f])
+    fill(c, d)
+    return c

@@ -1,0 +1,1 @@
+// Test infrastructure only: empty stand-in; the include at fdtd_plrc.t:10 is unused.

@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark of the MPulse time-stepping path on B200.
+
+Workload: PLRC + Kerr + CPML at 256 x 256 x 512 cells (two-pole Lorentz medium
+with chi3 E0^2 = 0.01 for z >= 64, 12-cell CPML on all six faces, focused
+Gaussian pulse injected by the paraxial short-pulse closed form), FP32 device
+state.  One "step" is one MPulse time step (E half + B half) over the whole
+grid.  The metric is Gcell-updates/s = nx ny nz x steps / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is timed with CUDA events on the simulation's stream, state resident in
+HBM (4.7 GB, larger than the 126 MB L2, so no L2 flush is needed).  `e2e` is the
+same metric through the C ABI with host buffers: upload of the six fields from
+pinned host memory, K steps, download of E, all inside the timed region.
+The FP64 form runs the same steps beside it, and the relative L2 error of the
+FP32 fields against it is reported.  With N > 1 every rank runs its own
+independent simulation (replicas only: the path is not sharded).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from mpulse_b200 import abi, configs  # noqa: E402
+
+WORKLOAD = dict(nx=256, ny=256, nz=512)
+WORKLOAD_NAME = "plrc_kerr_cpml_focused_256x256x512"
+METRIC = "Gcell-updates/s FP32 vs FP64 at rel-L2<=1e-5; adjoint/forward time ratio"
+UNIT = "Gcell-updates/s"
+# Process::time at which the timed steps start: the pulse is being injected then.
+START_TIME = 700
+
+
+def bench_config(precision: int) -> abi.Config:
+    return configs.c3_plrc_kerr(precision=precision, **WORKLOAD)
+
+
+def algorithmic_bytes(cfg: abi.Config, elem: int) -> dict:
+    """Algorithmic HBM bytes per step: every state element read once and written
+    once; neighbours, coefficient lines and source planes are free.
+        step:   s [12 N + 12 P N_med + 8 N_cpml]
+        E half: s [ 9 N + 12 P N_med + 4 N_cpml]   (E r/w, B r, psi r/w, psi_E r/w)
+        B half: s [ 9 N + 4 N_cpml]                 (B r/w, E r, psi_H r/w)
+    N_cpml counts face-slab cells per face (overlapping corners once per face)."""
+    N = cfg.nx * cfg.ny * cfg.nz
+    P = sum(1 for n in range(3) if cfg.poles[n].eps != 0)
+    z0 = max(cfg.medium_z0, 1)
+    z1 = min(cfg.medium_z1, cfg.nz)
+    Nmed = max(0, z1 - z0 + 1) * cfg.nx * cfg.ny
+    d = cfg.cpml_d
+    if cfg.cpml == abi.MP_CPML_ALL:
+        Ncpml = d * (2 * cfg.ny * cfg.nz + 2 * cfg.nx * cfg.nz + 2 * cfg.nx * cfg.ny)
+    elif cfg.cpml == abi.MP_CPML_Z:
+        Ncpml = d * 2 * cfg.nx * cfg.ny
+    else:
+        Ncpml = 0
+    return {
+        "step": elem * (12 * N + 12 * P * Nmed + 8 * Ncpml),
+        "e_half": elem * (9 * N + 12 * P * Nmed + 4 * Ncpml),
+        "b_half": elem * (9 * N + 4 * Ncpml),
+        "N": N, "P": P, "N_med": Nmed, "N_cpml": Ncpml,
+    }
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="clk_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_steps(sim, torch, steps: int, stream) -> tuple[float, int]:
+    """Device time (s) of `steps` steps with CUDA events on the sim's stream."""
+    L0 = sim.launches
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    sim.step_async(steps)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    sim.check_status()
+    return start.elapsed_time(stop) / 1e3, sim.launches - L0
+
+
+def run_ours(args) -> dict:
+    import torch
+    from mpulse_b200 import runtime
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    else:
+        torch.cuda.set_device(0)
+
+    cfg = bench_config(abi.MP_FP32)
+    cfg.device = local_rank
+    stream = torch.cuda.Stream()
+    sim = runtime.Simulation(cfg)
+    sim.set_stream(stream.cuda_stream)
+    sim.time = START_TIME
+    # warm-up
+    sim.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        dt_dev, launches = time_steps(sim, torch, args.steps, stream)
+    clocks = clk.summary()
+    barrier()
+    t_max = dt_dev
+    if dist is not None:
+        t = torch.tensor([dt_dev], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    cells = cfg.nx * cfg.ny * cfg.nz
+    value = world * cells * args.steps / t_max / 1e9
+
+    # per-kernel split: E half alone (B half and sources measured by difference)
+    kt = sim.kernel_times(max(3, min(args.steps, 10)))
+    alg = algorithmic_bytes(cfg, 4)
+    peaks = measured_peaks()
+    e_ms = kt["e_half_ms"]
+    achieved = alg["e_half"] / (e_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_e_half.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": "e_half_kernel<float,PLRC_NONLIN,2>", "achieved": round(achieved, 1),
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": traffic, "peak_source": peaks["source"],
+                "algorithmic_bytes_per_launch": alg["e_half"], "launch_ms": round(e_ms, 4)}
+    step_achieved = alg["step"] / (t_max / args.steps) / 1e9
+    step_roofline = {"achieved": round(step_achieved, 1), "frac": round(step_achieved / peaks["hbm_gbs"], 4),
+                     "algorithmic_bytes_per_step": alg["step"], "unit": "GB/s"}
+
+    # FP64 form on the same steps, and the FP32 error against it
+    fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
+    sim.close()
+    torch.cuda.empty_cache()
+    cfg64 = bench_config(abi.MP_FP64)
+    cfg64.device = local_rank
+    sim64 = runtime.Simulation(cfg64)
+    sim64.set_stream(stream.cuda_stream)
+    sim64.time = START_TIME
+    sim64.step(args.warmup)
+    dt64, _ = time_steps(sim64, torch, args.steps, stream)
+    fp64_state = {n: sim64.download(n) for n in ("Ex", "Ey", "Ez")}
+    sim64.close()
+    num = sum(float(np.sum((fp32_state[n] - fp64_state[n]) ** 2)) for n in fp32_state)
+    den = sum(float(np.sum(fp64_state[n] ** 2)) for n in fp64_state)
+    rel = math.sqrt(num / den) if den > 0 else None
+    value64 = world * cells * args.steps / dt64 / 1e9
+
+    # end to end through the C ABI with host buffers
+    e2e = run_e2e(args, torch, stream, local_rank)
+
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "grid": [cfg.nx, cfg.ny, cfg.nz], "solver": "fdtd-plrc-nonlin",
+                   "poles": 2, "cpml": "all faces, d=12", "source": "short_pulse_inject (focused, waist 2 um)",
+                   "start_time": START_TIME, "parallelism": f"replicas{world}",
+                   "l2": "state 4.7 GB > 126 MB L2, no flush needed"},
+        "fp64": {"value": round(value64, 4), "unit": UNIT, "ms_per_step": round(dt64 / args.steps * 1e3, 4)},
+        "fp32_over_fp64": round(value / value64, 3) if value64 > 0 else None,
+        "rel_l2_fp32_vs_fp64": rel,
+        "adjoint_forward_ratio": None,
+        "roofline": roofline, "step_roofline": step_roofline,
+        "kernel_ms": kt,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if args.cpu_baseline and rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline_sample(args)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out if rank == 0 else None
+
+
+def run_profile(args) -> dict:
+    """FP32 workload only: warm-up, then the timed steps; no other kernels."""
+    import torch
+    from mpulse_b200 import runtime
+    torch.cuda.set_device(0)
+    cfg = bench_config(abi.MP_FP32)
+    stream = torch.cuda.Stream()
+    sim = runtime.Simulation(cfg)
+    sim.set_stream(stream.cuda_stream)
+    sim.time = START_TIME
+    sim.step(args.warmup)
+    dt, launches = time_steps(sim, torch, args.steps, stream)
+    cells = cfg.nx * cfg.ny * cfg.nz
+    sim.close()
+    return {"profile_run": True, "grid": [cfg.nx, cfg.ny, cfg.nz], "steps": args.steps,
+            "value": cells * args.steps / dt / 1e9, "unit": UNIT, "gpu_launches": launches}
+
+
+def run_e2e(args, torch, stream, local_rank) -> dict:
+    from mpulse_b200 import runtime
+    cfg = bench_config(abi.MP_FP32)
+    cfg.device = local_rank
+    count = cfg.field_count()
+    host_in = {n: torch.zeros(count, dtype=torch.float64, pin_memory=True).numpy() for n in abi.FIELD_NAMES}
+    host_out = {n: torch.zeros(count, dtype=torch.float64, pin_memory=True).numpy() for n in ("Ex", "Ey", "Ez")}
+    sim = runtime.Simulation(cfg)
+    sim.set_stream(stream.cuda_stream)
+    sim.time = START_TIME
+    sim.step(1)  # first launch out of the timed region
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for n in abi.FIELD_NAMES:
+        sim.upload(n, host_in[n])
+    sim.step(args.steps)
+    for n in ("Ex", "Ey", "Ez"):
+        sim.download(n, host_out[n])
+    t1 = time.perf_counter()
+    sim.close()
+    cells = cfg.nx * cfg.ny * cfg.nz
+    return {"value": round(cells * args.steps / (t1 - t0) / 1e9, 4), "unit": UNIT,
+            "h2d_bytes_per_step": int(6 * count * 8 / args.steps), "d2h_bytes_per_step": int(3 * count * 8 / args.steps),
+            "what": "mp_upload x6 (pinned double) + mp_step(K) + mp_download x3, wall clock"}
+
+
+# ---------------------------------------------------------------------------
+# The reference on the host cores.
+
+def _ref_binary():
+    for name in ("mpulse_ref_fast", "mpulse_ref"):
+        p = os.path.join(ROOT, "oracle", "_ref", name)
+        if os.path.exists(p):
+            return p
+    return None
+
+
+def reference_slabs(steps: int, warmup: int, procs: int) -> dict:
+    """Runs the reference build on the bench workload split into `procs`
+    independent z-slabs (MPulse's own slab decomposition without the halo
+    exchange, one process per core, as its MPI build would run them) for
+    warmup + steps steps, and returns the aggregate rate of the timed steps."""
+    from oracle import pyoracle
+    binary = _ref_binary()
+    cfg = bench_config(abi.MP_FP64)
+    nz_slab = max(2 * cfg.cpml_d, cfg.nz // procs)
+    procs = max(1, cfg.nz // nz_slab)
+    tmp = tempfile.mkdtemp(prefix="mpref_bench_")
+    runs = []
+    for p in range(procs):
+        c = bench_config(abi.MP_FP64)
+        c.nz = nz_slab
+        c.medium_z0 = 0 if p > 0 else cfg.medium_z0
+        c.medium_z1 = nz_slab + 1
+        d = os.path.join(tmp, f"r{p}")
+        os.makedirs(d)
+        with open(os.path.join(d, "setup.dat"), "w") as f:
+            f.write(pyoracle.setup_text(c, warmup + steps))
+        env = dict(os.environ, MPULSE_REF_WARMUP=str(warmup))
+        runs.append((subprocess.Popen([binary, os.path.join(d, "setup.dat"), d], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, env=env, text=True), c))
+    secs, cells = [], 0
+    for pr, c in runs:
+        outp, _ = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError("reference run failed")
+        r = json.loads(outp.strip().splitlines()[-1])
+        secs.append(r["seconds"])
+        cells += r["cells"]
+    t = max(secs)
+    return {"value": cells * steps / t / 1e9, "procs": procs, "cells": cells, "seconds": t, "nz_slab": nz_slab}
+
+
+def cpu_baseline_sample(args) -> dict:
+    """Bounded CPU baseline for the headline line: the reference build on the
+    host cores for 2 timed steps of the full workload, split into z-slabs."""
+    if _ref_binary() is None:
+        return cpu_baseline_port()
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    r = reference_slabs(steps=2, warmup=1, procs=procs)
+    return {"value": round(r["value"], 6), "unit": UNIT, "cores": r["procs"], "kind": "reference",
+            "sample": f"MPulse reference build (-O3), full 256x256x512 workload as {r['procs']} independent "
+                      f"z-slabs of {r['nz_slab']} planes, 1 warm-up + 2 timed steps"}
+
+
+def cpu_baseline_port() -> dict:
+    from oracle import pyoracle
+    c = bench_config(abi.MP_FP64)
+    c.nz = 32
+    c.medium_z0 = 0
+    o = pyoracle.OracleSim(c)
+    o.time = START_TIME
+    t0 = time.perf_counter()
+    o.step(2)
+    t = time.perf_counter() - t0
+    return {"value": round(c.nx * c.ny * c.nz * 2 / t / 1e9, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "C oracle, 256x256x32 slab of the workload, 2 steps"}
+
+
+def run_reference_arm(args) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    if _ref_binary() is None:
+        return {"impl": "reference", "unavailable": "reference build missing (make -C oracle ref)"}
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    t0 = time.perf_counter()
+    r = reference_slabs(steps=args.steps, warmup=args.warmup, procs=procs)
+    wall = time.perf_counter() - t0
+    v = round(r["value"], 6)
+    sample = (f"MPulse reference build (-O3), the {WORKLOAD_NAME} workload as {r['procs']} independent z-slab "
+              f"processes of {r['nz_slab']} planes, {args.warmup} warm-up + {args.steps} timed steps")
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(r["seconds"] / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "grid": [256, 256, 512], "parallelism": f"{r['procs']} processes"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["procs"], "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(wall, 2),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="only the FP32 warm-up and timed steps (for ncu captures)")
+    ap.add_argument("--nz", type=int, default=None, help="override nz (smaller case for ncu --set full)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.nz:
+        WORKLOAD["nz"] = args.nz
+    if args.profile_only:
+        out = run_profile(args)
+    else:
+        out = run_reference_arm(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

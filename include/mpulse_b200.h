@@ -232,6 +232,14 @@ int mp_device_field(mp_ctx *ctx, const char *name, void **dptr, size_t *count,
 /* Number of CUDA kernel launches the context has issued so far. */
 long long mp_launch_count(mp_ctx *ctx);
 
+/* Advances the simulation by n_steps steps like mp_step while timing every
+ * kernel with CUDA events on the context's stream; returns the average device
+ * time of one launch of the E half-step kernel, of the B half-step kernel and
+ * of all source-plane kernels of one step together, in milliseconds.  Used for
+ * the per-kernel roofline; no counterpart in MPulse. */
+int mp_kernel_times(mp_ctx *ctx, int n_steps, double *e_half_ms, double *b_half_ms,
+                    double *sources_ms);
+
 /* Copies the message of the last failure (or "") into buf. */
 int mp_last_error(mp_ctx *ctx, char *buf, size_t n);
 

@@ -1,0 +1,864 @@
+// mp_api.cu - host side of the C ABI declared in include/mpulse_b200.h.
+//
+// It builds, once per context, everything MPulse recomputes or re-derives on
+// the host: the kappa lines (CPMLBorder[OneD]::initCoefficients,
+// cpml_border.cpp:58-139, :179-243), the CPML b/c coefficients
+// (CPMLBorderCurrent::makeCoeff, cpml_border.cpp:287-339), the PLRC recursion
+// coefficients (fdtd_plrc.t:181-216, FP64, identical every step because dt is
+// fixed) and the injector constants (sources.cpp:14-56,
+// shortpulseinject.cpp:56-113), and then drives the kernels of
+// mp_step_kernels.cu / mp_source_kernels.cu in MPulse's per-step order.
+#include "mpulse_b200.h"
+
+#include "mp_device.h"
+#include "mp_pulse_math.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace mpb {
+template <typename T> cudaError_t launch_e_half(const EParams<T> &, int, int, cudaStream_t);
+template <typename T> cudaError_t launch_b_half(const BParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_source_plane(const SourceEvalParams &, T *, T *, cudaStream_t);
+cudaError_t launch_convert_in(const double *src, void *dst, int fp32, long long n, int stride, int offset,
+                              cudaStream_t st);
+cudaError_t launch_convert_out(const void *src, double *dst, int fp32, long long n, int stride, int offset,
+                               cudaStream_t st);
+}  // namespace mpb
+
+using namespace mpb;
+
+namespace {
+
+const int kFaceOrderAll[6] = {FACE_NORTH, FACE_SOUTH, FACE_EAST, FACE_WEST, FACE_UP, FACE_DOWN};
+const int kFaceOrderZ[2] = {FACE_UP, FACE_DOWN};
+thread_local char g_create_err[512];
+
+int face_dim(int f) { return (f == FACE_EAST || f == FACE_WEST) ? 0 : (f == FACE_NORTH || f == FACE_SOUTH) ? 1 : 2; }
+bool face_low(int f) { return f == FACE_WEST || f == FACE_SOUTH || f == FACE_DOWN; }
+
+struct LayerHost {
+  int active = 0, dim = 0, lo = 0, hi = -1, zlo = 0, ex = 0, ey = 0;
+  size_t n = 0;
+  void *psi0 = nullptr, *psi1 = nullptr;
+  size_t b_off = 0, c_off = 0;  // offsets (elements) into the line buffer
+};
+
+}  // namespace
+
+struct mp_ctx {
+  mp_config cfg;
+  int fp32 = 0;
+  int esz = 8;
+  int mode = MODE_PLRC_LIN;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  long long plane = 0;
+  size_t fcount = 0;
+  void *F[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int np = 0;
+  int slot_of_pole[3] = {-1, -1, -1};
+  int mz0 = 1, mz1 = 0;
+  size_t psi_cells = 0;
+  void *psi[3][3] = {{nullptr}};
+  void *lines = nullptr;
+  LayerHost cpE[6], cpH[6];
+  int nsrc = 0;
+  SourceEvalParams sq[MP_MAX_SOURCES][2];
+  int src_plane[MP_MAX_SOURCES][2];
+  void *src_buf = nullptr;
+  double *d_wcoef = nullptr;
+  int *d_status = nullptr;
+  int *h_status = nullptr;
+  double *staging = nullptr;
+  size_t staging_n = 0;
+  long long time = 0;
+  long long launches = 0;
+  int pending_status = MP_OK;
+  std::string err;
+  EParams<float> epf;
+  BParams<float> bpf;
+  EParams<double> epd;
+  BParams<double> bpd;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int set_err(mp_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  else snprintf(g_create_err, sizeof g_create_err, "%s", buf);
+  return code;
+}
+
+int cuda_err(mp_ctx *c, cudaError_t e, const char *what) {
+  return set_err(c, e == cudaErrorMemoryAllocation ? MP_ERR_NO_MEMORY : MP_ERR_CUDA, "%s: %s", what,
+                 cudaGetErrorString(e));
+}
+
+cudaError_t dalloc(mp_ctx *c, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return e;
+  c->allocs.push_back(*p);
+  return cudaMemsetAsync(*p, 0, bytes, c->stream);
+}
+
+// Kappa lines exactly as CPMLBorder::initCoefficients (cpml_border.cpp:100-139)
+// and CPMLBorderOneD::initCoefficients (cpml_border.cpp:208-243).
+void kappa_lines(const mp_config &c, std::vector<double> kapE[3], std::vector<double> kapH[3]) {
+  const int n[3] = {c.nx, c.ny, c.nz};
+  const int d = c.cpml_d;
+  for (int a = 0; a < 3; ++a) {
+    kapE[a].assign(n[a] + 2, 1.0);
+    kapH[a].assign(n[a] + 2, 1.0);
+  }
+  auto grade = [&](double x) { return 1 + (c.cpml_kappa_max - 1) * x * x * x; };
+  if (c.cpml == MP_CPML_ALL) {
+    for (int a = 0; a < 3; ++a) {
+      const int low = 0, high = n[a] + 1;
+      for (int i = 0; i <= d; ++i) kapE[a][low + i] = grade(1 - double(i) / double(d));
+      for (int i = 0; i < d; ++i) kapH[a][low + i] = grade(1 - (double(i) + 0.5) / double(d));
+      for (int i = 0; i <= d; ++i) kapH[a][high - i] = grade(1 - double(i) / double(d));
+      for (int i = 0; i < d; ++i) kapE[a][high - i] = grade(1 - (double(i) + 0.5) / double(d));
+    }
+  } else if (c.cpml == MP_CPML_Z) {
+    const int low = 0, high = n[2] + 1;
+    for (int i = 0; i < d; ++i) kapE[2][low + i + 1] = grade(1 - double(i) / double(d));
+    for (int i = 0; i < d; ++i) kapH[2][low + i] = grade(1 - (double(i) + 0.5) / double(d));
+    for (int i = 0; i < d; ++i) kapE[2][high - i - 1] = grade(1 - double(i) / double(d));
+    for (int i = 0; i < d; ++i) kapH[2][high - i - 1] = grade(1 - double(i + 0.5) / double(d));
+  }
+}
+
+int validate(const mp_config *c) {
+  if (!c) return set_err(nullptr, MP_ERR_INVALID, "config is NULL");
+  if (c->abi_version != MP_ABI_VERSION)
+    return set_err(nullptr, MP_ERR_INVALID, "abi_version %d, library speaks %d", c->abi_version, MP_ABI_VERSION);
+  if (c->nx < 2 || c->ny < 2 || c->nz < 2) return set_err(nullptr, MP_ERR_INVALID, "grid must be at least 2 cells per axis");
+  if (!(c->dx > 0 && c->dy > 0 && c->dz > 0 && c->dt > 0))
+    return set_err(nullptr, MP_ERR_INVALID, "grid spacings and dt must be positive");
+  if (c->precision != MP_FP64 && c->precision != MP_FP32) return set_err(nullptr, MP_ERR_INVALID, "unknown precision");
+  if (c->solver < MP_SOLVER_PLAIN || c->solver > MP_SOLVER_PLRC_NONLIN)
+    return set_err(nullptr, MP_ERR_INVALID, "unknown solver %d", c->solver);
+  if (c->boundary != MP_BOUNDARY_PERIODIC && c->boundary != MP_BOUNDARY_XY_PERIODIC)
+    return set_err(nullptr, MP_ERR_INVALID, "unknown boundary %d", c->boundary);
+  const bool plrc = c->solver == MP_SOLVER_PLRC_LIN || c->solver == MP_SOLVER_PLRC_NONLIN;
+  if (!plrc && (c->cpml != MP_CPML_NONE || c->n_sources > 0))
+    return set_err(nullptr, MP_ERR_INVALID,
+                   "additional currents cannot be used with this field solver (fieldsolver.h:198-216)");
+  if (plrc) {
+    for (int n = 0; n < MP_MAX_POLES; ++n) {
+      if (c->poles[n].om2 == 0)
+        return set_err(nullptr, MP_ERR_INVALID, "FDTD_PLRCSolver: Omega should not be zero! (pole %d)", n + 1);
+      if (!(c->poles[n].om2 > c->poles[n].delta * c->poles[n].delta))
+        return set_err(nullptr, MP_ERR_INVALID, "pole %d needs om2 > delta^2", n + 1);
+    }
+    if (!(c->eps_bg != 0) || !std::isfinite(c->eps_bg)) return set_err(nullptr, MP_ERR_INVALID, "eps_bg must be non-zero");
+  }
+  if (c->cpml != MP_CPML_NONE) {
+    if (c->cpml != MP_CPML_ALL && c->cpml != MP_CPML_Z) return set_err(nullptr, MP_ERR_INVALID, "unknown cpml kind");
+    if (c->cpml_d < 1) return set_err(nullptr, MP_ERR_INVALID, "cpml_d must be >= 1");
+    const int lim = c->cpml == MP_CPML_Z ? c->nz : std::min(c->nx, std::min(c->ny, c->nz));
+    if (c->cpml_d > lim) return set_err(nullptr, MP_ERR_INVALID, "CPML thicker (%d) than the domain (%d)", c->cpml_d, lim);
+    if (c->cpml_sigma_max == 0 && c->cpml_a_max == 0)
+      return set_err(nullptr, MP_ERR_INVALID, "CPML with sigmaMax = aMax = 0 has undefined c = 0/0 (cpml_border.cpp:333)");
+  }
+  if (c->n_sources < 0 || c->n_sources > MP_MAX_SOURCES) return set_err(nullptr, MP_ERR_INVALID, "n_sources out of range");
+  for (int s = 0; s < c->n_sources; ++s) {
+    const mp_source &q = c->sources[s];
+    if (q.kind == MP_SOURCE_FOCUSED_PULSE)
+      return set_err(nullptr, MP_ERR_UNSUPPORTED, "focused_pulse_inject is not built");
+    if (q.kind < MP_SOURCE_PLANE_WAVE || q.kind > MP_SOURCE_SHORT_PULSE)
+      return set_err(nullptr, MP_ERR_INVALID, "source %d: unknown kind %d", s, q.kind);
+    if (q.distance < 1 || q.distance > c->nz)
+      return set_err(nullptr, MP_ERR_INVALID, "source %d: distance %d outside 1..nz", s, q.distance);
+    if (!(q.eps > 0)) return set_err(nullptr, MP_ERR_INVALID, "source %d: eps must be positive", s);
+  }
+  if (c->newton_max_iter < 1) return set_err(nullptr, MP_ERR_INVALID, "newton_max_iter must be >= 1");
+  return MP_OK;
+}
+
+template <typename T>
+void fill_face(CpmlFace<T> &F, const LayerHost &L, const T *lines) {
+  F.active = L.active;
+  F.dim = L.dim;
+  F.lo = L.lo;
+  F.hi = L.hi;
+  F.zlo = L.zlo;
+  F.ex = L.ex;
+  F.ey = L.ey;
+  F.psi0 = static_cast<T *>(L.psi0);
+  F.psi1 = static_cast<T *>(L.psi1);
+  F.b = lines + L.b_off;
+  F.c = lines + L.c_off;
+}
+
+template <typename T>
+void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<size_t> &ikE_off,
+                  const std::vector<size_t> &ikH_off, size_t bzy_off, const double coef[3][3][2], double numer,
+                  double denom) {
+  const mp_config &g = c->cfg;
+  const T *lines = static_cast<const T *>(c->lines);
+  ep = EParams<T>();
+  bp = BParams<T>();
+  ep.nx = bp.nx = g.nx;
+  ep.ny = bp.ny = g.ny;
+  ep.nz = bp.nz = g.nz;
+  ep.plane = bp.plane = c->plane;
+  for (int a = 0; a < 3; ++a) {
+    ep.E[a] = static_cast<T *>(c->F[a]);
+    ep.B[a] = static_cast<const T *>(c->F[3 + a]);
+    bp.E[a] = static_cast<const T *>(c->F[a]);
+    bp.B[a] = static_cast<T *>(c->F[3 + a]);
+    ep.ik[a] = lines + ikE_off[a];
+    bp.ik[a] = lines + ikH_off[a];
+  }
+  bp.ik_bz_y = lines + bzy_off;
+  const bool zper = g.boundary == MP_BOUNDARY_PERIODIC;
+  ep.zperiodic = bp.zperiodic = zper ? 1 : 0;
+  ep.k_first = 1;
+  ep.k_last = (c->mode == MODE_PLAIN || c->mode == MODE_NL) && !zper ? g.nz + 1 : g.nz;
+  bp.k_first = zper ? 1 : 0;
+  bp.k_last = g.nz;
+  ep.dt = bp.dt = T(g.dt);
+  ep.mz0 = c->mz0;
+  ep.mz1 = c->mz1;
+  for (int s = 0; s < c->np; ++s)
+    for (int a = 0; a < 3; ++a) ep.psi[s][a] = static_cast<T *>(c->psi[s][a]);
+  for (int s = 0; s < 3; ++s)
+    for (int q = 0; q < 2; ++q) {
+      ep.pD[s][q] = T(coef[0][s][q]);
+      ep.pxi[s][q] = T(coef[1][s][q]);
+      ep.pC[s][q] = T(coef[2][s][q]);
+    }
+  ep.numer = T(numer);
+  ep.inv_denom = T(1.0 / denom);
+  ep.eps_bg = T(g.eps_bg);
+  ep.inv_eps_bg = T(1.0 / g.eps_bg);
+  ep.chi_over_denom = g.chi / denom;
+  ep.chi = T(g.chi);
+  ep.eps_d = g.eps;
+  ep.chi_d = g.chi;
+  ep.newton_tol = g.newton_tol;
+  ep.newton_max = g.newton_max_iter;
+  for (int f = 0; f < 6; ++f) {
+    fill_face(ep.cpml[f], c->cpE[f], lines);
+    fill_face(bp.cpml[f], c->cpH[f], lines);
+  }
+  ep.n_src = bp.n_src = c->nsrc;
+  const size_t pl = size_t(c->plane);
+  for (int s = 0; s < c->nsrc; ++s) {
+    T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * pl;
+    ep.src[s].plane = c->src_plane[s][0];
+    ep.src[s].v0 = base;
+    ep.src[s].v1 = base + pl;
+    bp.src[s].plane = c->src_plane[s][1];
+    bp.src[s].v0 = base + 2 * pl;
+    bp.src[s].v1 = base + 3 * pl;
+  }
+  ep.status = c->d_status;
+  // planes per block: enough blocks to fill 148 SMs several times over
+  const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+  const long long target = 148LL * 8;
+  const int ne = ep.k_last - ep.k_first + 1, nb = bp.k_last - bp.k_first + 1;
+  const long long chunks = std::max(1LL, (target + blocks_xy - 1) / blocks_xy);
+  ep.kchunk = int(std::max(1LL, (ne + chunks - 1) / chunks));
+  bp.kchunk = int(std::max(1LL, (nb + chunks - 1) / chunks));
+}
+
+int create_impl(const mp_config *cfg, mp_ctx **out) {
+  int rc = validate(cfg);
+  if (rc != MP_OK) return rc;
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) return set_err(nullptr, MP_ERR_CUDA, "cudaSetDevice(%d): %s", cfg->device, cudaGetErrorString(e));
+
+  mp_ctx *c = new (std::nothrow) mp_ctx();
+  if (!c) return set_err(nullptr, MP_ERR_NO_MEMORY, "out of host memory");
+  c->cfg = *cfg;
+  const mp_config &g = c->cfg;
+  c->fp32 = g.precision == MP_FP32;
+  c->esz = c->fp32 ? 4 : 8;
+  c->mode = g.solver == MP_SOLVER_PLAIN ? MODE_PLAIN
+            : g.solver == MP_SOLVER_NL  ? MODE_NL
+            : g.solver == MP_SOLVER_PLRC_LIN ? MODE_PLRC_LIN
+                                             : MODE_PLRC_NONLIN;
+  e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { rc = cuda_err(nullptr, e, "cudaStreamCreate"); delete c; return rc; }
+  c->stream = c->own_stream;
+  c->plane = (long long)g.nx * g.ny;
+  c->fcount = size_t(g.nz + 2) * size_t(c->plane);
+
+  auto fail = [&](int code) {
+    snprintf(g_create_err, sizeof g_create_err, "%s", c->err.c_str());
+    mp_destroy(c);
+    return code;
+  };
+#define MPB_TRY(expr, what)                          \
+  do {                                               \
+    cudaError_t e_ = (expr);                         \
+    if (e_ != cudaSuccess) return fail(cuda_err(c, e_, what)); \
+  } while (0)
+
+  for (int f = 0; f < 6; ++f) MPB_TRY(dalloc(c, &c->F[f], c->fcount * c->esz), "field allocation");
+
+  const bool plrc = c->mode == MODE_PLRC_LIN || c->mode == MODE_PLRC_NONLIN;
+  // PLRC: active poles (Delta eps != 0) and their accumulators over the medium
+  // planes the E update touches.  A pole with Delta eps = 0 has dchi0 = dxi0 = 0
+  // and an accumulator that stays 0 from MPulse's zero start, so it is skipped.
+  double coef[3][3][2] = {{{0}}};  // [D, dxi0, Crec][slot][re, im]
+  double numer = g.eps, denom = g.eps;
+  if (plrc) {
+    c->mz0 = std::max(g.medium_z0, 1);
+    c->mz1 = std::min(g.medium_z1, g.nz);
+    // FDTD_PLRCSolver::stepD coefficient block (fdtd_plrc.t:181-216)
+    const std::complex<double> I(0, 1);
+    std::complex<double> sumChi = 0.0, sumXi = 0.0;
+    for (int n = 0; n < 3; ++n) {
+      const mp_lorentz_pole &P = g.poles[n];
+      const double beta = std::sqrt(P.om2 - P.delta * P.delta);
+      const double gamma = P.eps * P.om2 / beta;
+      const std::complex<double> phasor = P.delta - I * beta;
+      const std::complex<double> Crec = std::exp(-phasor * g.dt);
+      const std::complex<double> chi0 = (I * gamma * (Crec - 1.0) / phasor);
+      const std::complex<double> xi0 = I * gamma * (Crec * (phasor * g.dt + 1.0) - 1.0) / (phasor * phasor * g.dt);
+      const std::complex<double> dchi0 = chi0 * (1.0 - Crec), dxi0 = xi0 * (1.0 - Crec);
+      sumChi += chi0;
+      sumXi += xi0;
+      if (P.eps != 0.0 && c->mz0 <= c->mz1) {
+        const int s = c->np++;
+        c->slot_of_pole[n] = s;
+        const std::complex<double> D = dchi0 - dxi0;
+        coef[0][s][0] = D.real(); coef[0][s][1] = D.imag();
+        coef[1][s][0] = dxi0.real(); coef[1][s][1] = dxi0.imag();
+        coef[2][s][0] = Crec.real(); coef[2][s][1] = Crec.imag();
+      }
+    }
+    const double sumChi0 = sumChi.real(), sumXi0 = sumXi.real();
+    numer = g.eps - sumXi0 - 0.0;
+    denom = (c->mode == MODE_PLRC_LIN) ? g.eps + (sumChi0 - sumXi0) + 0.0 : g.eps + sumChi0 - sumXi0 + 0.0;
+    if (c->mz0 <= c->mz1) {
+      c->psi_cells = size_t(c->mz1 - c->mz0 + 1) * size_t(c->plane);
+      for (int s = 0; s < c->np; ++s)
+        for (int a = 0; a < 3; ++a) MPB_TRY(dalloc(c, &c->psi[s][a], 2 * c->psi_cells * c->esz), "psi allocation");
+    }
+  }
+
+  // Lines: ikE[3], ikH[3], bz_y, then b/c per CPML face (E 6, H 6), each the
+  // full axis length n+2, all in one buffer of T.
+  std::vector<double> kapE[3], kapH[3];
+  kappa_lines(g, kapE, kapH);
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  const double d3[3] = {g.dx, g.dy, g.dz};
+  std::vector<double> host_lines;
+  std::vector<size_t> ikE_off(3), ikH_off(3);
+  for (int a = 0; a < 3; ++a) {
+    ikE_off[a] = host_lines.size();
+    for (int i = 0; i < n3[a] + 2; ++i) host_lines.push_back(1.0 / (kapE[a][i] * d3[a]));
+  }
+  for (int a = 0; a < 3; ++a) {
+    ikH_off[a] = host_lines.size();
+    for (int i = 0; i < n3[a] + 2; ++i) host_lines.push_back(1.0 / (kapH[a][i] * d3[a]));
+  }
+  const size_t bzy_off = host_lines.size();
+  for (int i = 0; i < g.ny + 2; ++i)
+    host_lines.push_back(plrc ? 1.0 / (kapH[1][i] * g.dy) : 1.0 / g.dx);  // fdtd_plain.cpp:115 divides by dx
+
+  const int kb0 = g.boundary == MP_BOUNDARY_PERIODIC ? 1 : 0;
+  if (g.cpml != MP_CPML_NONE) {
+    const int *order = g.cpml == MP_CPML_ALL ? kFaceOrderAll : kFaceOrderZ;
+    const int nface = g.cpml == MP_CPML_ALL ? 6 : 2;
+    const int d = g.cpml_d;
+    for (int q = 0; q < nface; ++q) {
+      const int f = order[q];
+      const int dim = face_dim(f);
+      const int n = n3[dim];
+      for (int isH = 0; isH < 2; ++isH) {
+        LayerHost &L = isH ? c->cpH[q] : c->cpE[q];
+        // the reference layer along dim (getBorderExtent with the distances of
+        // cpml_border.cpp:353 and :441-450)
+        const int distance = (isH && face_low(f)) ? 0 : 1;
+        int rlo, rhi;
+        if (face_low(f)) { rlo = distance; rhi = d - 1 + distance; }
+        else { rlo = n + 1 - d + 1 - distance; rhi = n + 1 - distance; }
+        // b and c (makeCoeff), positions counted from the outer edge
+        std::vector<double> bl(n + 2, 0.0), cl(n + 2, 0.0);
+        const double offset = isH ? 0.5 : 0.0;
+        for (int k = 0; k < d; ++k) {
+          const double x = 1 - (double(k) - offset) / double(d);
+          const double x3 = x * x * x;
+          const int pos = face_low(f) ? (rlo + k) : (rhi - k);
+          const double sigma = x3 * g.cpml_sigma_max;
+          const double kappa = 1 + (g.cpml_kappa_max - 1) * x3;
+          const double a = g.cpml_a_max * (1 - x);
+          const double b = std::exp(-(sigma / kappa + a) * g.dt / 1.0);
+          const double cc = sigma * (b - 1) / (kappa * (sigma + kappa * a));
+          bl[pos] = b;
+          cl[pos] = cc / d3[dim];
+        }
+        // restrict to the cells the kernels update
+        int ulo, uhi;
+        if (dim == 2) { ulo = isH ? kb0 : 1; uhi = g.nz; }
+        else { ulo = 1; uhi = n; }
+        L.dim = dim;
+        L.lo = std::max(rlo, ulo);
+        L.hi = std::min(rhi, uhi);
+        L.active = L.lo <= L.hi;
+        if (!L.active) continue;
+        L.zlo = isH ? kb0 : 1;
+        const int zdepth = g.nz - L.zlo + 1;
+        L.ex = dim == 0 ? L.hi - L.lo + 1 : g.nx;
+        L.ey = dim == 1 ? L.hi - L.lo + 1 : g.ny;
+        const int ez = dim == 2 ? L.hi - L.lo + 1 : zdepth;
+        L.n = size_t(L.ex) * L.ey * ez;
+        MPB_TRY(dalloc(c, &L.psi0, L.n * c->esz), "CPML allocation");
+        MPB_TRY(dalloc(c, &L.psi1, L.n * c->esz), "CPML allocation");
+        L.b_off = host_lines.size();
+        host_lines.insert(host_lines.end(), bl.begin(), bl.end());
+        L.c_off = host_lines.size();
+        host_lines.insert(host_lines.end(), cl.begin(), cl.end());
+      }
+    }
+  }
+
+  // Incident sources.
+  std::vector<double> wcoef(kFaddeevaTerms);
+  double wL = 0;
+  faddeeva_coefficients(wcoef.data(), &wL);
+  MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_wcoef), wcoef.size() * sizeof(double)), "source allocation");
+  MPB_TRY(cudaMemcpyAsync(c->d_wcoef, wcoef.data(), wcoef.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+          "cudaMemcpy");
+  c->nsrc = g.n_sources;
+  for (int s = 0; s < g.n_sources; ++s) {
+    const mp_source &q = g.sources[s];
+    for (int isH = 0; isH < 2; ++isH) {
+      SourceEvalParams &p = c->sq[s][isH];
+      p = SourceEvalParams();
+      p.kind = q.kind;
+      p.nx = g.nx;
+      p.ny = g.ny;
+      p.isH = isH;
+      p.l = q.distance - 1;
+      p.dx = g.dx; p.dy = g.dy; p.dz = g.dz; p.dt = g.dt;
+      p.DX = g.dz;
+      if (q.kind == MP_SOURCE_PLANE_WAVE || q.kind == MP_SOURCE_PLANE_GAUSS) {
+        // PlaneWaveSource::makeECurrent (sources.cpp:14-34)
+        const double *k = q.k, *H = q.H;
+        double E[3] = {k[1] * H[2] - k[2] * H[1], k[2] * H[0] - k[0] * H[2], k[0] * H[1] - k[1] * H[0]};
+        const double bmag = std::sqrt(H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
+        const double factor = -bmag / std::sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+        for (int a = 0; a < 3; ++a) {
+          p.k[a] = k[a];
+          p.amp3[a] = isH ? E[a] * (factor / std::sqrt(q.eps)) : H[a];
+          p.bg[a] = isH ? q.E_bg[a] : q.H_bg[a];
+        }
+        p.om = std::sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]) / std::sqrt(q.eps);
+        p.ramp = q.ramp;
+        p.width = q.width;
+        p.offset = q.offset;
+      } else {
+        // ShortPulseInjectSourceFunc::setParam (shortpulseinject.cpp:56-113)
+        p.centre[0] = 0.5 * double(g.nx + 1);
+        p.centre[1] = 0.5 * double(g.ny + 1);
+        p.centre[2] = 0.5 * double(g.nz + 1);
+        p.lightspeed = std::sqrt(1 / q.eps);
+        p.ZRl = 0.5 * q.om0 * q.waist * q.waist / p.lightspeed;
+        p.length = q.length;
+        p.om0 = q.om0;
+        ShortPulse sp;
+        sp.c = p.lightspeed; sp.ZRl = p.ZRl; sp.phase = 0.0; sp.T = q.length; sp.om0 = q.om0;
+        sp.coef = wcoef.data(); sp.L = wL;
+        const double Exmax = short_pulse_e(sp, 0, 0, 0, 0).re;
+        p.amp = q.amp / Exmax;
+        p.phase = 2 * M_PI * q.phase;
+        p.tshift = q.t_shift;
+        p.zshift = q.z_shift;
+        p.w_coef = c->d_wcoef;
+        p.w_L = wL;
+      }
+    }
+    c->src_plane[s][0] = q.distance;      // E current layer z = d
+    c->src_plane[s][1] = q.distance - 1;  // H current layer z = d - 1 (incsource.t:91)
+  }
+  if (c->nsrc) MPB_TRY(dalloc(c, &c->src_buf, size_t(c->nsrc) * 4 * size_t(c->plane) * c->esz), "source allocation");
+
+  // upload the lines
+  MPB_TRY(dalloc(c, &c->lines, host_lines.size() * c->esz), "line allocation");
+  if (c->fp32) {
+    std::vector<float> hf(host_lines.begin(), host_lines.end());
+    MPB_TRY(cudaMemcpyAsync(c->lines, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice, c->stream), "cudaMemcpy");
+    MPB_TRY(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  } else {
+    MPB_TRY(cudaMemcpyAsync(c->lines, host_lines.data(), host_lines.size() * 8, cudaMemcpyHostToDevice, c->stream),
+            "cudaMemcpy");
+    MPB_TRY(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  }
+  MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_status), ST_COUNT * sizeof(int)), "status allocation");
+  MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_status), ST_COUNT * sizeof(int)), "pinned allocation");
+
+  if (c->fp32) build_params<float>(c, c->epf, c->bpf, ikE_off, ikH_off, bzy_off, coef, numer, denom);
+  else build_params<double>(c, c->epd, c->bpd, ikE_off, ikH_off, bzy_off, coef, numer, denom);
+  MPB_TRY(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+#undef MPB_TRY
+  *out = c;
+  return MP_OK;
+}
+
+// Resolves a field name to (device pointer, stride, offset, first plane,
+// number of planes) of its device array.
+struct FieldView {
+  void *base = nullptr;
+  int stride = 1, offset = 0;
+  int k0 = 0, nk = 0;
+  bool zero = false;  // a pole without state: reads as zeros
+};
+
+int resolve(mp_ctx *c, const char *name, FieldView &v) {
+  static const char *fn[6] = {"Ex", "Ey", "Ez", "Bx", "By", "Bz"};
+  if (!name) return set_err(c, MP_ERR_NAME, "field name is NULL");
+  for (int f = 0; f < 6; ++f)
+    if (!strcmp(name, fn[f])) {
+      v.base = c->F[f];
+      v.k0 = 0;
+      v.nk = c->cfg.nz + 2;
+      return MP_OK;
+    }
+  if (!strncmp(name, "Psi", 3) && (name[3] == 'R' || name[3] == 'I') && name[4] >= '1' && name[4] <= '3' &&
+      name[5] >= 'x' && name[5] <= 'z' && name[6] == 0) {
+    const bool plrc = c->mode == MODE_PLRC_LIN || c->mode == MODE_PLRC_NONLIN;
+    if (!plrc) return set_err(c, MP_ERR_NAME, "%s: solver has no PLRC accumulators", name);
+    const int pole = name[4] - '1', comp = name[5] - 'x';
+    const int s = c->slot_of_pole[pole];
+    v.stride = 2;
+    v.offset = name[3] == 'R' ? 0 : 1;
+    if (s < 0) {
+      v.zero = true;
+      return MP_OK;
+    }
+    v.base = c->psi[s][comp];
+    v.k0 = c->mz0;
+    v.nk = c->mz1 - c->mz0 + 1;
+    return MP_OK;
+  }
+  return set_err(c, MP_ERR_NAME, "unknown field name '%s'", name);
+}
+
+int ensure_staging(mp_ctx *c, size_t n) {
+  if (c->staging_n >= n) return MP_OK;
+  if (c->staging) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_n = 0;
+  }
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&c->staging), n * sizeof(double));
+  if (e != cudaSuccess) return cuda_err(c, e, "staging allocation");
+  c->staging_n = n;
+  return MP_OK;
+}
+
+const size_t kStagingChunk = size_t(1) << 24;  // doubles per host<->device chunk
+
+// Optional per-kernel event timing (mp_kernel_times): events recorded before
+// and after each group of launches of one step.
+struct StepTimer {
+  cudaEvent_t ev[6];
+  bool on = false;
+};
+
+template <typename T>
+int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer *tm = nullptr,
+              double *acc = nullptr) {
+  for (int t = 0; t < n_steps; ++t) {
+    cudaError_t e;
+    if (tm) cudaEventRecord(tm->ev[0], c->stream);
+    for (int s = 0; s < c->nsrc; ++s) {
+      c->sq[s][0].time = c->time;
+      T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * size_t(c->plane);
+      e = launch_source_plane<T>(c->sq[s][0], base, base + c->plane, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
+      c->launches++;
+    }
+    if (tm) cudaEventRecord(tm->ev[1], c->stream);
+    e = launch_e_half<T>(ep, c->mode, c->np, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "E half-step kernel");
+    c->launches++;
+    if (tm) cudaEventRecord(tm->ev[2], c->stream);
+    for (int s = 0; s < c->nsrc; ++s) {
+      c->sq[s][1].time = c->time;
+      T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * size_t(c->plane);
+      e = launch_source_plane<T>(c->sq[s][1], base + 2 * c->plane, base + 3 * c->plane, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
+      c->launches++;
+    }
+    if (tm) cudaEventRecord(tm->ev[3], c->stream);
+    e = launch_b_half<T>(bp, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "B half-step kernel");
+    c->launches++;
+    if (tm) {
+      cudaEventRecord(tm->ev[4], c->stream);
+      e = cudaEventSynchronize(tm->ev[4]);
+      if (e != cudaSuccess) return cuda_err(c, e, "event synchronize");
+      float ms[4];
+      for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&ms[q], tm->ev[q], tm->ev[q + 1]);
+      acc[0] += ms[1];          // E half
+      acc[1] += ms[3];          // B half
+      acc[2] += ms[0] + ms[2];  // sources
+    }
+    c->time++;
+  }
+  return MP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mp_config_defaults(mp_config *c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->abi_version = MP_ABI_VERSION;
+  c->nx = c->ny = c->nz = 32;
+  c->dx = c->dy = c->dz = 0.1;  // grid-dx.. default (globals.cpp:57-59)
+  c->dt = 1e-2;                 // dt default (globals.cpp:61)
+  c->precision = MP_FP64;
+  c->solver = MP_SOLVER_PLRC_LIN;
+  c->boundary = MP_BOUNDARY_PERIODIC;
+  c->eps = 1.0;   // fdtd_plrc.t:417
+  c->chi = 0.1;   // fdtd_plrc.cpp:463, fdtd_nl.cpp:151
+  for (int n = 0; n < MP_MAX_POLES; ++n) {
+    c->poles[n].eps = 0.0;    // fdtd_plrc.t:419-421
+    c->poles[n].delta = 0.0;  // :423-425
+    c->poles[n].om2 = 1.0;    // :427-429
+  }
+  c->medium_z0 = 0;
+  c->medium_z1 = 1 << 30;
+  c->eps_bg = 1.0;
+  c->cpml = MP_CPML_NONE;
+  c->cpml_d = 8;              // cpml_border.cpp:146-149
+  c->cpml_kappa_max = 15.0;
+  c->cpml_a_max = 0.25;
+  c->cpml_sigma_max = 3.0;
+  c->n_sources = 0;
+  for (int s = 0; s < MP_MAX_SOURCES; ++s) {
+    mp_source &q = c->sources[s];
+    q.kind = MP_SOURCE_NONE;
+    q.distance = 15;          // incsource.cpp:84
+    q.k[2] = 1.0;             // sources.cpp:64
+    q.ramp = 0.5;             // sources.cpp:78
+    q.width = 10.0;           // sources.cpp:237
+    q.offset = 40.0;          // sources.cpp:238
+    q.eps = 1.0;
+    q.length = 1.0;           // shortpulseinject.cpp:38-46
+    q.waist = 1.0;
+    q.om0 = 2 * M_PI;
+    q.amp = 1.0;
+  }
+  c->newton_max_iter = 64;
+  c->newton_tol = 1e-9;       // fdtd_plrc.cpp:414
+  c->device = 0;
+}
+
+int mp_create(const mp_config *cfg, mp_ctx **out) {
+  if (!out) return set_err(nullptr, MP_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  g_create_err[0] = 0;
+  return create_impl(cfg, out);
+}
+
+const char *mp_create_error(void) { return g_create_err; }
+
+void mp_destroy(mp_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->staging) cudaFree(c->staging);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+int mp_set_stream(mp_ctx *c, void *s) {
+  if (!c) return MP_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamSynchronize");
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
+  return MP_OK;
+}
+
+int mp_field_size(mp_ctx *c, const char *name, size_t *count) {
+  if (!c || !count) return MP_ERR_INVALID;
+  FieldView v;
+  int rc = resolve(c, name, v);
+  if (rc != MP_OK) return rc;
+  *count = c->fcount;
+  return MP_OK;
+}
+
+int mp_upload(mp_ctx *c, const char *name, const double *host, size_t count) {
+  if (!c || !host) return MP_ERR_INVALID;
+  FieldView v;
+  int rc = resolve(c, name, v);
+  if (rc != MP_OK) return rc;
+  if (count != c->fcount) return set_err(c, MP_ERR_INVALID, "%s: %zu values, expected %zu", name, count, c->fcount);
+  cudaSetDevice(c->cfg.device);
+  if (v.zero) {
+    for (size_t q = 0; q < count; ++q)
+      if (host[q] != 0.0) return set_err(c, MP_ERR_INVALID, "%s: this pole has Delta eps = 0 and keeps no state", name);
+    return MP_OK;
+  }
+  const size_t pl = size_t(c->plane);
+  const size_t n = size_t(v.nk) * pl;
+  const double *src = host + size_t(v.k0) * pl;
+  rc = ensure_staging(c, std::min(n, kStagingChunk));
+  if (rc != MP_OK) return rc;
+  for (size_t off = 0; off < n; off += kStagingChunk) {
+    const size_t m = std::min(kStagingChunk, n - off);
+    cudaError_t e = cudaMemcpyAsync(c->staging, src + off, m * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "upload copy");
+    char *dst = static_cast<char *>(v.base) + off * size_t(v.stride) * c->esz;
+    e = launch_convert_in(c->staging, dst, c->fp32, (long long)m, v.stride, v.offset, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "upload convert");
+    c->launches++;
+  }
+  return MP_OK;
+}
+
+int mp_download(mp_ctx *c, const char *name, double *host, size_t count) {
+  if (!c || !host) return MP_ERR_INVALID;
+  FieldView v;
+  int rc = resolve(c, name, v);
+  if (rc != MP_OK) return rc;
+  if (count != c->fcount) return set_err(c, MP_ERR_INVALID, "%s: %zu values, expected %zu", name, count, c->fcount);
+  cudaSetDevice(c->cfg.device);
+  const size_t pl = size_t(c->plane);
+  if (v.zero || v.nk < int(c->cfg.nz + 2)) memset(host, 0, count * sizeof(double));
+  if (!v.zero) {
+    const size_t n = size_t(v.nk) * pl;
+    double *dstbase = host + size_t(v.k0) * pl;
+    rc = ensure_staging(c, std::min(n, kStagingChunk));
+    if (rc != MP_OK) return rc;
+    for (size_t off = 0; off < n; off += kStagingChunk) {
+      const size_t m = std::min(kStagingChunk, n - off);
+      const char *src = static_cast<const char *>(v.base) + off * size_t(v.stride) * c->esz;
+      cudaError_t e = launch_convert_out(src, c->staging, c->fp32, (long long)m, v.stride, v.offset, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "download convert");
+      c->launches++;
+      e = cudaMemcpyAsync(dstbase + off, c->staging, m * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "download copy");
+    }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "download");
+  }
+  // z-periodic grids: the ghost planes are images (periodic_bound.cpp:53-71)
+  const bool field = name[0] == 'E' || name[0] == 'B';
+  if (field && c->cfg.boundary == MP_BOUNDARY_PERIODIC) {
+    const int nz = c->cfg.nz;
+    memcpy(host, host + size_t(nz) * pl, pl * sizeof(double));
+    memcpy(host + size_t(nz + 1) * pl, host + pl, pl * sizeof(double));
+  }
+  return MP_OK;
+}
+
+int mp_step_async(mp_ctx *c, int n_steps) {
+  if (!c || n_steps < 0) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  return c->fp32 ? step_impl<float>(c, c->epf, c->bpf, n_steps) : step_impl<double>(c, c->epd, c->bpd, n_steps);
+}
+
+int mp_check_status(mp_ctx *c) {
+  if (!c) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  cudaError_t e = cudaMemcpyAsync(c->h_status, c->d_status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "status read");
+  const int newton = c->h_status[ST_NEWTON], nonfin = c->h_status[ST_NONFINITE];
+  if (newton || nonfin) {
+    cudaMemsetAsync(c->d_status, 0, ST_COUNT * sizeof(int), c->stream);
+    if (nonfin) return set_err(c, MP_ERR_NONFINITE, "%d field values became NaN or Inf", nonfin);
+    return set_err(c, MP_ERR_NEWTON, "Kerr Newton solve did not converge in %d cell updates (max %d iterations)",
+                   newton, c->cfg.newton_max_iter);
+  }
+  return MP_OK;
+}
+
+int mp_step(mp_ctx *c, int n_steps) {
+  int rc = mp_step_async(c, n_steps);
+  if (rc != MP_OK) return rc;
+  return mp_check_status(c);
+}
+
+int mp_get_time(mp_ctx *c, long long *t) {
+  if (!c || !t) return MP_ERR_INVALID;
+  *t = c->time;
+  return MP_OK;
+}
+
+int mp_set_time(mp_ctx *c, long long t) {
+  if (!c) return MP_ERR_INVALID;
+  c->time = t;
+  return MP_OK;
+}
+
+int mp_sync(mp_ctx *c) {
+  if (!c) return MP_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? MP_OK : cuda_err(c, e, "cudaStreamSynchronize");
+}
+
+int mp_device_field(mp_ctx *c, const char *name, void **dptr, size_t *count, int *elem_bytes) {
+  if (!c || !dptr || !count || !elem_bytes) return MP_ERR_INVALID;
+  FieldView v;
+  int rc = resolve(c, name, v);
+  if (rc != MP_OK) return rc;
+  if (v.stride != 1) return set_err(c, MP_ERR_NAME, "%s: accumulators are stored complex-interleaved", name);
+  *dptr = v.base;
+  *count = c->fcount;
+  *elem_bytes = c->esz;
+  return MP_OK;
+}
+
+long long mp_launch_count(mp_ctx *c) { return c ? c->launches : -1; }
+
+int mp_kernel_times(mp_ctx *c, int n_steps, double *e_ms, double *b_ms, double *s_ms) {
+  if (!c || n_steps < 1 || !e_ms || !b_ms || !s_ms) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  StepTimer tm;
+  for (int q = 0; q < 6; ++q) {
+    cudaError_t e = cudaEventCreate(&tm.ev[q]);
+    if (e != cudaSuccess) return cuda_err(c, e, "cudaEventCreate");
+  }
+  double acc[3] = {0, 0, 0};
+  int rc = c->fp32 ? step_impl<float>(c, c->epf, c->bpf, n_steps, &tm, acc)
+                   : step_impl<double>(c, c->epd, c->bpd, n_steps, &tm, acc);
+  for (int q = 0; q < 6; ++q) cudaEventDestroy(tm.ev[q]);
+  if (rc != MP_OK) return rc;
+  *e_ms = acc[0] / n_steps;
+  *b_ms = acc[1] / n_steps;
+  *s_ms = acc[2] / n_steps;
+  return mp_check_status(c);
+}
+
+int mp_last_error(mp_ctx *c, char *buf, size_t n) {
+  if (!buf || n == 0) return MP_ERR_INVALID;
+  const char *m = c ? c->err.c_str() : g_create_err;
+  snprintf(buf, n, "%s", m);
+  return MP_OK;
+}
+
+}  // extern "C"

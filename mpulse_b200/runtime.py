@@ -1,0 +1,183 @@
+"""ctypes binding of the C ABI in include/mpulse_b200.h (libmpulse_b200.so).
+
+``Simulation`` is a thin object wrapper over one ``mp_ctx``: the host-side
+counterpart of MPulse's FieldSimulation + FieldSolver pair for the
+time-stepping path (src/fieldsim.cpp:31-112, src/fieldsolver.h:10-37).  There is
+no CPU fallback: if the library is missing or no GPU is present, creating a
+Simulation raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpulse_b200.so")
+
+# Every entry point include/mpulse_b200.h declares.
+EXPORTED = (
+    "mp_config_defaults", "mp_create", "mp_destroy", "mp_set_stream", "mp_field_size",
+    "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
+    "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
+    "mp_last_error", "mp_create_error", "mp_kernel_times",
+)
+
+_lib = None
+
+
+class MPulseError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libmpulse_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m mpulse_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, cp, sz, dp = C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_double)
+    L.mp_config_defaults.argtypes = [C.POINTER(abi.Config)]
+    L.mp_config_defaults.restype = None
+    L.mp_create.argtypes = [C.POINTER(abi.Config), C.POINTER(vp)]
+    L.mp_create.restype = C.c_int
+    L.mp_destroy.argtypes = [vp]
+    L.mp_destroy.restype = None
+    L.mp_set_stream.argtypes = [vp, vp]
+    L.mp_set_stream.restype = C.c_int
+    L.mp_field_size.argtypes = [vp, cp, C.POINTER(sz)]
+    L.mp_field_size.restype = C.c_int
+    L.mp_upload.argtypes = [vp, cp, dp, sz]
+    L.mp_upload.restype = C.c_int
+    L.mp_download.argtypes = [vp, cp, dp, sz]
+    L.mp_download.restype = C.c_int
+    for f in (L.mp_step, L.mp_step_async):
+        f.argtypes = [vp, C.c_int]
+        f.restype = C.c_int
+    L.mp_check_status.argtypes = [vp]
+    L.mp_check_status.restype = C.c_int
+    L.mp_get_time.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.mp_get_time.restype = C.c_int
+    L.mp_set_time.argtypes = [vp, C.c_longlong]
+    L.mp_set_time.restype = C.c_int
+    L.mp_sync.argtypes = [vp]
+    L.mp_sync.restype = C.c_int
+    L.mp_device_field.argtypes = [vp, cp, C.POINTER(vp), C.POINTER(sz), C.POINTER(C.c_int)]
+    L.mp_device_field.restype = C.c_int
+    L.mp_launch_count.argtypes = [vp]
+    L.mp_launch_count.restype = C.c_longlong
+    L.mp_last_error.argtypes = [vp, C.c_char_p, sz]
+    L.mp_last_error.restype = C.c_int
+    L.mp_kernel_times.argtypes = [vp, C.c_int, dp, dp, dp]
+    L.mp_kernel_times.restype = C.c_int
+    L.mp_create_error.argtypes = []
+    L.mp_create_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def library_defaults() -> abi.Config:
+    c = abi.Config()
+    lib().mp_config_defaults(C.byref(c))
+    return c
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Simulation:
+    """One simulation held in HBM (an ``mp_ctx``)."""
+
+    def __init__(self, cfg: abi.Config):
+        L = lib()
+        self.cfg = cfg
+        h = C.c_void_p()
+        rc = L.mp_create(C.byref(cfg), C.byref(h))
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, L.mp_create_error().decode())
+        self._h = h
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- errors
+    def last_error(self) -> str:
+        buf = C.create_string_buffer(512)
+        lib().mp_last_error(self._h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc: int):
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, self.last_error())
+
+    # -- fields
+    def upload(self, name: str, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        self._check(lib().mp_upload(self._h, name.encode(), _dptr(a), a.size))
+
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.cfg.field_count(), dtype=np.float64)
+        self._check(lib().mp_download(self._h, name.encode(), _dptr(out), out.size))
+        return out.reshape(self.cfg.field_shape())
+
+    def device_field(self, name: str):
+        p, n, es = C.c_void_p(), C.c_size_t(), C.c_int()
+        self._check(lib().mp_device_field(self._h, name.encode(), C.byref(p), C.byref(n), C.byref(es)))
+        return p.value, n.value, es.value
+
+    # -- stepping
+    def step(self, n: int = 1):
+        self._check(lib().mp_step(self._h, int(n)))
+
+    def step_async(self, n: int = 1):
+        self._check(lib().mp_step_async(self._h, int(n)))
+
+    def check_status(self):
+        self._check(lib().mp_check_status(self._h))
+
+    def sync(self):
+        self._check(lib().mp_sync(self._h))
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(lib().mp_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    @property
+    def time(self) -> int:
+        t = C.c_longlong()
+        self._check(lib().mp_get_time(self._h, C.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, t: int):
+        self._check(lib().mp_set_time(self._h, int(t)))
+
+    def kernel_times(self, n: int) -> dict:
+        """Runs n steps with per-kernel CUDA-event timing; average ms per launch."""
+        e, b, s = C.c_double(), C.c_double(), C.c_double()
+        self._check(lib().mp_kernel_times(self._h, int(n), C.byref(e), C.byref(b), C.byref(s)))
+        return {"e_half_ms": e.value, "b_half_ms": b.value, "sources_ms": s.value}
+
+    @property
+    def launches(self) -> int:
+        return lib().mp_launch_count(self._h)

@@ -18,6 +18,7 @@
 //     of the step loop alone is printed as one JSON line.
 //
 // Usage: mpulse_ref SETUP OUTDIR [grid names...]
+// Environment: MPULSE_REF_WARMUP=W times only the steps after the first W.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -204,14 +205,19 @@ int main(int argc, char **argv) {
   process->Rebuild(setup);
   process->init();
 
+  // MPULSE_REF_WARMUP=W leaves the first W steps out of the timing.
   const int T = Globals::instance().totalTime();
-  const auto t0 = std::chrono::steady_clock::now();
+  const char *w = std::getenv("MPULSE_REF_WARMUP");
+  const int warm = w ? std::atoi(w) : 0;
+  auto t0 = std::chrono::steady_clock::now();
   for (process->time = 0; process->time < T; ++process->time) {
+    if (process->time == warm) t0 = std::chrono::steady_clock::now();
     process->fieldSim->execute();
     DiagnosticManager::instance().execute();
   }
   const auto t1 = std::chrono::steady_clock::now();
   const double seconds = std::chrono::duration<double>(t1 - t0).count();
+  const int timed = T > warm ? T - warm : T;
 
   Storage &st = *process->fieldSim;
   for (int a = 3; a < argc; ++a) writeGrid(argv[2], argv[a], st.getGrid(argv[a]));
@@ -219,8 +225,8 @@ int main(int argc, char **argv) {
   const GridIndex lo = st.getLow(), hi = st.getHigh();
   const long long cells = (long long)(hi[0] - lo[0] - 1) * (hi[1] - lo[1] - 1) * (hi[2] - lo[2] - 1);
   std::cout.rdbuf(coutBuf);
-  std::printf("{\"steps\": %d, \"cells\": %lld, \"seconds\": %.9f, \"low\": [%d, %d, %d], \"high\": [%d, %d, %d]}\n",
-              T, cells, seconds, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
+  std::printf("{\"steps\": %d, \"timed_steps\": %d, \"cells\": %lld, \"seconds\": %.9f, \"low\": [%d, %d, %d], \"high\": [%d, %d, %d]}\n",
+              T, timed, cells, seconds, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
   std::fflush(stdout);
   // The reference never frees its plug-ins; skip teardown the same way.
   std::_Exit(0);

@@ -1,0 +1,72 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry point
+the header declares, its struct layout and defaults agree with the Python
+mirror, and invalid configurations are rejected with an error code (never an
+exit) before any device work."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from mpulse_b200 import abi, runtime
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "mpulse_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mp_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = runtime.lib()
+    names = declared_functions()
+    assert names, "no declarations found"
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in include/mpulse_b200.h but not exported"
+    assert set(names) == set(runtime.EXPORTED)
+
+
+def test_defaults_match_python_mirror():
+    a = bytes(runtime.library_defaults())
+    b = bytes(abi.default_config())
+    assert len(a) == C.sizeof(abi.Config)
+    assert a == b
+
+
+def _create_error(cfg):
+    L = runtime.lib()
+    h = C.c_void_p()
+    rc = L.mp_create(C.byref(cfg), C.byref(h))
+    return rc, L.mp_create_error().decode()
+
+
+@pytest.mark.parametrize("mutate,code,text", [
+    (lambda c: setattr(c, "abi_version", 99), abi.MP_ERR_INVALID, "abi_version"),
+    (lambda c: setattr(c, "nx", 1), abi.MP_ERR_INVALID, "at least 2"),
+    (lambda c: setattr(c, "dt", 0.0), abi.MP_ERR_INVALID, "positive"),
+    (lambda c: setattr(c.poles[1], "om2", 0.0), abi.MP_ERR_INVALID, "Omega should not be zero"),
+    (lambda c: (setattr(c.poles[0], "delta", 2.0), setattr(c.poles[0], "om2", 1.0)), abi.MP_ERR_INVALID, "om2 > delta"),
+    (lambda c: (setattr(c, "cpml", abi.MP_CPML_ALL), setattr(c, "cpml_d", 40)), abi.MP_ERR_INVALID, "thicker"),
+    (lambda c: (setattr(c, "cpml", abi.MP_CPML_Z), setattr(c, "cpml_sigma_max", 0.0), setattr(c, "cpml_a_max", 0.0)),
+     abi.MP_ERR_INVALID, "0/0"),
+    (lambda c: (setattr(c, "solver", abi.MP_SOLVER_PLAIN), setattr(c, "cpml", abi.MP_CPML_Z)), abi.MP_ERR_INVALID,
+     "cannot be used"),
+    (lambda c: (setattr(c, "n_sources", 1), setattr(c.sources[0], "kind", abi.MP_SOURCE_PLANE_GAUSS),
+                setattr(c.sources[0], "distance", 0)), abi.MP_ERR_INVALID, "distance"),
+    (lambda c: setattr(c, "solver", 9), abi.MP_ERR_INVALID, "unknown solver"),
+])
+def test_invalid_configs_are_rejected(mutate, code, text):
+    cfg = abi.default_config()
+    mutate(cfg)
+    rc, msg = _create_error(cfg)
+    assert rc == code
+    assert text in msg
+
+
+def test_null_arguments():
+    L = runtime.lib()
+    assert L.mp_create(None, None) == abi.MP_ERR_INVALID
+    assert L.mp_step(None, 1) == abi.MP_ERR_INVALID
+    assert L.mp_launch_count(None) == -1

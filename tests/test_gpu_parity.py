@@ -1,0 +1,113 @@
+"""CUDA path vs the FP64 CPU oracle on the same seeded inputs, through the C ABI.
+
+FP64 form: relative L2 error <= 1e-12 per field (the oracle reproduces the
+reference bit for bit, see test_oracle_reference.py).  FP32 form: relative L2
+error <= 1e-5 against the FP64 oracle (the precision target of the FP32 form).
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+from mpulse_b200 import abi, runtime
+from oracle import pyoracle
+from tests.cases import CASES, make_case, random_fields, rel_l2
+
+TOL_FP64 = 1e-12
+TOL_FP32 = 1e-5
+STEPS = 25
+
+pytestmark = pytest.mark.gpu
+
+
+def run_pair(cfg, init, steps, names=abi.FIELD_NAMES):
+    o = pyoracle.OracleSim(cfg)
+    for n, v in init.items():
+        o.upload(n, v)
+    rc = o.step(steps)
+    assert rc == abi.MP_OK
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.step(steps)
+        assert g.time == steps
+        got = {n: g.download(n) for n in names}
+    want = {n: o.download(n) for n in names}
+    return got, want
+
+
+def psi_names(cfg):
+    if cfg.solver not in (abi.MP_SOLVER_PLRC_LIN, abi.MP_SOLVER_PLRC_NONLIN):
+        return ()
+    return tuple(f"Psi{ri}{n + 1}{c}" for ri in "RI" for n in range(3) if cfg.poles[n].eps != 0 for c in "xyz")
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fp64_matches_oracle(case):
+    cfg = make_case(case, abi.MP_FP64)
+    init = random_fields(cfg, seed=zlib.crc32(case.encode()) % 1000)
+    names = abi.FIELD_NAMES + psi_names(cfg)
+    got, want = run_pair(cfg, init, STEPS, names)
+    for n in names:
+        err = rel_l2(got[n], want[n])
+        assert err <= TOL_FP64, f"{case} {n}: rel-L2 {err:.3e}"
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fp32_matches_oracle(case):
+    cfg32 = make_case(case, abi.MP_FP32)
+    cfg64 = make_case(case, abi.MP_FP64)
+    init = random_fields(cfg64, seed=7 + zlib.crc32(case.encode()) % 1000, smooth=True)
+    o = pyoracle.OracleSim(cfg64)
+    for n, v in init.items():
+        o.upload(n, v)
+    o.step(STEPS)
+    with runtime.Simulation(cfg32) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.step(STEPS)
+        for n in abi.FIELD_NAMES:
+            err = rel_l2(g.download(n), o.download(n))
+            assert err <= TOL_FP32, f"{case} {n}: rel-L2 {err:.3e}"
+
+
+def test_upload_download_roundtrip_and_ghosts():
+    cfg = make_case("plain_periodic", abi.MP_FP64)
+    init = random_fields(cfg, seed=3)
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        for n, v in init.items():
+            np.testing.assert_array_equal(g.download(n), v)
+
+
+def test_newton_cap_reports_error_without_fault():
+    cfg = make_case("nonlin_one_pole_periodic", abi.MP_FP64)
+    cfg.chi = 50.0
+    cfg.newton_max_iter = 1
+    init = random_fields(cfg, seed=5, scale=2.0)
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        with pytest.raises(runtime.MPulseError) as ei:
+            g.step(2)
+        assert ei.value.code == abi.MP_ERR_NEWTON
+        # the context stays usable
+        cfg2 = make_case("nonlin_one_pole_periodic", abi.MP_FP64)
+        g2 = runtime.Simulation(cfg2)
+        g2.step(1)
+        g2.close()
+
+
+def test_time_counter_and_sources_follow_process_time():
+    """Setting the time moves the injected pulse exactly like Process::time."""
+    cfg = make_case("lin_split_cpmlz_gauss", abi.MP_FP64)
+    o = pyoracle.OracleSim(cfg)
+    o.time = 40
+    o.step(10)
+    with runtime.Simulation(cfg) as g:
+        g.time = 40
+        g.step(10)
+        assert g.time == 50
+        for n in abi.FIELD_NAMES:
+            assert rel_l2(g.download(n), o.download(n)) <= TOL_FP64

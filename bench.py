@@ -103,7 +103,8 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)  # let nvidia-smi start before the timed region
         except Exception:
             self.proc = None
         return self
@@ -195,8 +196,10 @@ def run_ours(args) -> dict:
         t_max = float(t.item())
     cells = cfg.nx * cfg.ny * cfg.nz
     value = world * cells * args.steps / t_max / 1e9
+    # FP32 state after warmup + steps, compared below with the FP64 form
+    fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
 
-    # per-kernel split: E half alone (B half and sources measured by difference)
+    # per-kernel device times (CUDA events around each launch, further steps)
     kt = sim.kernel_times(max(3, min(args.steps, 10)))
     alg = algorithmic_bytes(cfg, 4)
     peaks = measured_peaks()
@@ -216,7 +219,6 @@ def run_ours(args) -> dict:
                      "algorithmic_bytes_per_step": alg["step"], "unit": "GB/s"}
 
     # FP64 form on the same steps, and the FP32 error against it
-    fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
     sim.close()
     torch.cuda.empty_cache()
     cfg64 = bench_config(abi.MP_FP64)
@@ -406,7 +408,7 @@ def run_reference_arm(args) -> dict | None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -72,6 +72,7 @@ struct mp_ctx {
   void *lines = nullptr;
   LayerHost cpE[6], cpH[6];
   int nsrc = 0;
+  int src_mult = 0;
   SourceEvalParams sq[MP_MAX_SOURCES][2];
   int src_plane[MP_MAX_SOURCES][2];
   void *src_buf = nullptr;
@@ -261,6 +262,7 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
     fill_face(bp.cpml[f], c->cpH[f], lines);
   }
   ep.n_src = bp.n_src = c->nsrc;
+  ep.src_mult = bp.src_mult = c->src_mult;
   const size_t pl = size_t(c->plane);
   for (int s = 0; s < c->nsrc; ++s) {
     T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * pl;
@@ -425,6 +427,8 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
         L.ey = dim == 1 ? L.hi - L.lo + 1 : g.ny;
         const int ez = dim == 2 ? L.hi - L.lo + 1 : zdepth;
         L.n = size_t(L.ex) * L.ey * ez;
+        if (L.n >= (size_t(1) << 31))
+          return fail(set_err(c, MP_ERR_UNSUPPORTED, "CPML layer of %zu cells exceeds 2^31 (32-bit layer index)", L.n));
         MPB_TRY(dalloc(c, &L.psi0, L.n * c->esz), "CPML allocation");
         MPB_TRY(dalloc(c, &L.psi1, L.n * c->esz), "CPML allocation");
         L.b_off = host_lines.size();
@@ -442,9 +446,19 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_wcoef), wcoef.size() * sizeof(double)), "source allocation");
   MPB_TRY(cudaMemcpyAsync(c->d_wcoef, wcoef.data(), wcoef.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
           "cudaMemcpy");
-  c->nsrc = g.n_sources;
-  for (int s = 0; s < g.n_sources; ++s) {
-    const mp_source &q = g.sources[s];
+  // All built injector kinds use the `down` face, and every injector on a face
+  // shares the border-layer grids "IncidentEJx".. / "IncidentHJx".. of the first
+  // one (Storage::addBorderLayer returns the grid already registered under the
+  // name, storage.cpp:129-141).  Each injector's stepScheme overwrites the shared
+  // grid over the first injector's extent, and sumCurrents adds the grid once
+  // per injector: the step sees the LAST injector's field on the FIRST one's
+  // planes, n_sources times.  One plane pair is evaluated and added src_mult
+  // times.
+  c->nsrc = g.n_sources > 0 ? 1 : 0;
+  c->src_mult = g.n_sources;
+  for (int s = 0; s < c->nsrc; ++s) {
+    const mp_source &q = g.sources[g.n_sources - 1];
+    const mp_source &first = g.sources[0];
     for (int isH = 0; isH < 2; ++isH) {
       SourceEvalParams &p = c->sq[s][isH];
       p = SourceEvalParams();
@@ -452,7 +466,7 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
       p.nx = g.nx;
       p.ny = g.ny;
       p.isH = isH;
-      p.l = q.distance - 1;
+      p.l = first.distance - 1;
       p.dx = g.dx; p.dy = g.dy; p.dz = g.dz; p.dt = g.dt;
       p.DX = g.dz;
       if (q.kind == MP_SOURCE_PLANE_WAVE || q.kind == MP_SOURCE_PLANE_GAUSS) {
@@ -491,8 +505,8 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
         p.w_L = wL;
       }
     }
-    c->src_plane[s][0] = q.distance;      // E current layer z = d
-    c->src_plane[s][1] = q.distance - 1;  // H current layer z = d - 1 (incsource.t:91)
+    c->src_plane[s][0] = first.distance;      // E current layer z = d
+    c->src_plane[s][1] = first.distance - 1;  // H current layer z = d - 1 (incsource.t:91)
   }
   if (c->nsrc) MPB_TRY(dalloc(c, &c->src_buf, size_t(c->nsrc) * 4 * size_t(c->plane) * c->esz), "source allocation");
 

@@ -79,6 +79,7 @@ struct EParams {
 
   CpmlFace<T> cpml[6];    // E-side CPML currents in MPulse's current order
   int n_src;
+  int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
   int *status;
 };
@@ -97,6 +98,7 @@ struct BParams {
   const T *ik_bz_y;       // line used for dEx/dy in the Bz update
   CpmlFace<T> cpml[6];
   int n_src;
+  int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
 };
 

@@ -98,53 +98,72 @@ __global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
 
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * plane;
+    // ---- all loads of this cell first: the arrays may alias as far as the
+    // compiler knows, so a load placed after a store would wait for it
     const T bx = ld(Bx + base + col), by = ld(By + base + col), bz = ld(Bz + base + col);
     const T bz_xm = ld(Bz + base + colxm), by_xm = ld(By + base + colxm);
     const T bz_ym = ld(Bz + base + colym), bx_ym = ld(Bx + base + colym);
     const T ex = Ex[base + col], ey = Ey[base + col], ez = Ez[base + col];
-
-    T jx = T(0), jy = T(0), jz = T(0);
-    T ikz;
-    if (MODE == MODE_PLAIN || MODE == MODE_NL) {
-      ikz = ld(p.ik[2] + k);
-    } else {
-      ikz = ld(p.ik[2] + k);
-      // E-side CPML currents, summed in MPulse's current order (fdtd_plrc.t:352-373)
+    const T ikz = ld(p.ik[2] + k);
+    const bool med = (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) && k >= p.mz0 && k <= p.mz1;
+    const long long pi = ((long long)(k - p.mz0) * p.ny + j) * p.nx + i;
+    T2 q[NP > 0 ? NP : 1][3];
+    if (NP > 0 && med) {
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        const CpmlFace<T> &F = p.cpml[f];
-        if (!F.active) continue;
-        const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
-        if (idx < F.lo || idx > F.hi) continue;
-        long long li;
-        T d0, d1;  // differences of B along dim for psi0, psi1
-        if (F.dim == 2) {
-          li = ((long long)(k - F.lo) * p.ny + j) * p.nx + i;
-          d0 = -(by - by_km);
-          d1 = bx - bx_km;
-        } else if (F.dim == 0) {
-          li = ((long long)(k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
-          d0 = -(bz - bz_xm);
-          d1 = by - by_xm;
-        } else {
-          li = ((long long)(k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
-          d0 = -(bx - bx_ym);
-          d1 = bz - bz_ym;
-        }
-        const T b = ld(F.b + idx), c = ld(F.c + idx);
-        const T s0 = b * F.psi0[li] + c * d0;
-        const T s1 = b * F.psi1[li] + c * d1;
-        F.psi0[li] = s0;
-        F.psi1[li] = s1;
-        if (F.dim == 2) { jx += s0; jy += s1; }
-        else if (F.dim == 0) { jy += s0; jz += s1; }
-        else { jz += s0; jx += s1; }
+      for (int n = 0; n < NP; ++n)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) q[n][c] = reinterpret_cast<const T2 *>(p.psi[n][c])[pi];
+    }
+    T cp0[6], cp1[6], cb[6], cc[6];
+    int cli[6];  // layer arrays hold < 2^31 cells (checked by mp_create)
+    bool cin[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const CpmlFace<T> &F = p.cpml[f];
+      const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
+      cin[f] = (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) && F.active && idx >= F.lo && idx <= F.hi;
+      if (cin[f]) {
+        if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+        else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+        else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
+        cp0[f] = F.psi0[cli[f]];
+        cp1[f] = F.psi1[cli[f]];
+        cb[f] = ld(F.b + idx);
+        cc[f] = ld(F.c + idx);
       }
-      for (int s = 0; s < p.n_src; ++s) {
-        if (k == p.src[s].plane) {
-          jx += ld(p.src[s].v0 + col);
-          jy += ld(p.src[s].v1 + col);
-        }
+    }
+    T sa = T(0), sb = T(0);
+    bool on_src = false;
+    for (int s = 0; s < p.n_src; ++s) {
+      if (k == p.src[s].plane) {
+        sa = ld(p.src[s].v0 + col);
+        sb = ld(p.src[s].v1 + col);
+        on_src = true;
+      }
+    }
+
+    // ---- E-side currents, summed in MPulse's current order
+    // (fdtd_plrc.t:352-373): CPML faces (cpml_border.cpp:398-425), then the
+    // injector plane
+    T jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (!cin[f]) continue;
+      const int dim = p.cpml[f].dim;
+      T d0, d1;  // differences of B along dim for psi0, psi1
+      if (dim == 2) { d0 = -(by - by_km); d1 = bx - bx_km; }
+      else if (dim == 0) { d0 = -(bz - bz_xm); d1 = by - by_xm; }
+      else { d0 = -(bx - bx_ym); d1 = bz - bz_ym; }
+      cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
+      cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+      if (dim == 2) { jx += cp0[f]; jy += cp1[f]; }
+      else if (dim == 0) { jy += cp0[f]; jz += cp1[f]; }
+      else { jz += cp0[f]; jx += cp1[f]; }
+    }
+    if (on_src) {
+      for (int m = 0; m < p.src_mult; ++m) {
+        jx += sa;
+        jy += sb;
       }
     }
 
@@ -172,7 +191,6 @@ __global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
         exn = eyn = ezn = T(0);
       }
     } else {
-      const bool med = (k >= p.mz0) && (k <= p.mz1);
       if (!med) {
         // background: no poles, no Kerr term
         exn = (p.eps_bg * ex + dt * (cbx + jx)) * p.inv_eps_bg;
@@ -181,24 +199,19 @@ __global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
       } else {
         T Px = T(0), Py = T(0), Pz = T(0);
         if (NP > 0) {
-          const long long pi = ((long long)(k - p.mz0) * p.ny + j) * p.nx + i;
           const T e3[3] = {ex, ey, ez};
           T P3[3] = {T(0), T(0), T(0)};
 #pragma unroll
           for (int n = 0; n < NP; ++n) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              T2 *ps = reinterpret_cast<T2 *>(p.psi[n][c]) + pi;
-              const T2 q = *ps;
               // psi~ = (dchi0 - dxi0) e + psi ; Psi += Re psi~
-              const T ar = p.pD[n][0] * e3[c] + q.x;
-              const T ai = p.pD[n][1] * e3[c] + q.y;
+              const T ar = p.pD[n][0] * e3[c] + q[n][c].x;
+              const T ai = p.pD[n][1] * e3[c] + q[n][c].y;
               P3[c] += ar;
               // psi <- dxi0 e + Crec psi~
-              T2 r;
-              r.x = p.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
-              r.y = p.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
-              *ps = r;
+              q[n][c].x = p.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
+              q[n][c].y = p.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
             }
           }
           Px = P3[0]; Py = P3[1]; Pz = P3[2];
@@ -226,9 +239,22 @@ __global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
       }
     }
     if (!finite3((double)exn, (double)eyn, (double)ezn)) atomicAdd(p.status + ST_NONFINITE, 1);
+    // ---- all stores last
     Ex[base + col] = exn;
     Ey[base + col] = eyn;
     Ez[base + col] = ezn;
+    if (NP > 0 && med) {
+#pragma unroll
+      for (int n = 0; n < NP; ++n)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) reinterpret_cast<T2 *>(p.psi[n][c])[pi] = q[n][c];
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (!cin[f]) continue;
+      p.cpml[f].psi0[cli[f]] = cp0[f];
+      p.cpml[f].psi1[cli[f]] = cp1[f];
+    }
     bx_km = bx;
     by_km = by;
   }
@@ -273,48 +299,69 @@ __global__ void __launch_bounds__(256) b_half_kernel(const BParams<T> p) {
     const T ez_xp = ld(Ez + base + colxp), ey_xp = ld(Ey + base + colxp);
     const T ez_yp = ld(Ez + base + colyp), ex_yp = ld(Ex + base + colyp);
     const T ikz = ld(p.ik[2] + k);
-
-    T mx = T(0), my = T(0), mz = T(0);
+    // ---- all loads first (see e_half_kernel)
+    const T bx = Bx[base + col], by = By[base + col], bz = Bz[base + col];
+    T cp0[6], cp1[6], cb[6], cc[6];
+    int cli[6];  // layer arrays hold < 2^31 cells (checked by mp_create)
+    bool cin[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const CpmlFace<T> &F = p.cpml[f];
-      if (!F.active) continue;
       const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
-      if (idx < F.lo || idx > F.hi) continue;
-      long long li;
-      T d0, d1;
-      if (F.dim == 2) {
-        li = ((long long)(k - F.lo) * p.ny + j) * p.nx + i;
-        d0 = ey_kp - ey_k;
-        d1 = -(ex_kp - ex_k);
-      } else if (F.dim == 0) {
-        li = ((long long)(k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
-        d0 = ez_xp - ez;
-        d1 = -(ey_xp - ey_k);
-      } else {
-        li = ((long long)(k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
-        d0 = ex_yp - ex_k;
-        d1 = -(ez_yp - ez);
+      cin[f] = F.active && idx >= F.lo && idx <= F.hi;
+      if (cin[f]) {
+        if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+        else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+        else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
+        cp0[f] = F.psi0[cli[f]];
+        cp1[f] = F.psi1[cli[f]];
+        cb[f] = ld(F.b + idx);
+        cc[f] = ld(F.c + idx);
       }
-      const T b = ld(F.b + idx), c = ld(F.c + idx);
-      const T s0 = b * F.psi0[li] + c * d0;
-      const T s1 = b * F.psi1[li] + c * d1;
-      F.psi0[li] = s0;
-      F.psi1[li] = s1;
-      if (F.dim == 2) { mx += s0; my += s1; }
-      else if (F.dim == 0) { my += s0; mz += s1; }
-      else { mz += s0; mx += s1; }
     }
+    T sa = T(0), sb = T(0);
+    bool on_src = false;
     for (int s = 0; s < p.n_src; ++s) {
       if (k == p.src[s].plane) {
-        mx += ld(p.src[s].v0 + col);
-        my += ld(p.src[s].v1 + col);
+        sa = ld(p.src[s].v0 + col);
+        sb = ld(p.src[s].v1 + col);
+        on_src = true;
       }
     }
 
-    Bx[base + col] = Bx[base + col] + dt * ((ey_kp - ey_k) * ikz - (ez_yp - ez) * iky + mx);
-    By[base + col] = By[base + col] + dt * ((ez_xp - ez) * ikx - (ex_kp - ex_k) * ikz + my);
-    Bz[base + col] = Bz[base + col] + dt * ((ex_yp - ex_k) * iky_bz - (ey_xp - ey_k) * ikx + mz);
+    // ---- H-side currents (cpml_border.cpp:499-527, incsource.t:112-145)
+    T mx = T(0), my = T(0), mz = T(0);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (!cin[f]) continue;
+      const int dim = p.cpml[f].dim;
+      T d0, d1;
+      if (dim == 2) { d0 = ey_kp - ey_k; d1 = -(ex_kp - ex_k); }
+      else if (dim == 0) { d0 = ez_xp - ez; d1 = -(ey_xp - ey_k); }
+      else { d0 = ex_yp - ex_k; d1 = -(ez_yp - ez); }
+      cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
+      cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+      if (dim == 2) { mx += cp0[f]; my += cp1[f]; }
+      else if (dim == 0) { my += cp0[f]; mz += cp1[f]; }
+      else { mz += cp0[f]; mx += cp1[f]; }
+    }
+    if (on_src) {
+      for (int m = 0; m < p.src_mult; ++m) {
+        mx += sa;
+        my += sb;
+      }
+    }
+
+    // ---- plrcStepB (fdtd_plrc.cpp:263-293), stores last
+    Bx[base + col] = bx + dt * ((ey_kp - ey_k) * ikz - (ez_yp - ez) * iky + mx);
+    By[base + col] = by + dt * ((ez_xp - ez) * ikx - (ex_kp - ex_k) * ikz + my);
+    Bz[base + col] = bz + dt * ((ex_yp - ex_k) * iky_bz - (ey_xp - ey_k) * ikx + mz);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (!cin[f]) continue;
+      p.cpml[f].psi0[cli[f]] = cp0[f];
+      p.cpml[f].psi1[cli[f]] = cp1[f];
+    }
     ex_k = ex_kp;
     ey_k = ey_kp;
   }

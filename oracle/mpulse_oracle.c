@@ -516,6 +516,14 @@ static void add_inc_layers(mpo_sim *s, int n) {
     int distance = p->distance;
     if (isH && !reverse) distance = distance - 1;
     if (!border_extent(s, dir, 1, distance, &L->box)) continue;
+    /* Storage::addBorderLayer (storage.cpp:129-141) returns the grid already
+     * registered under "IncidentEJx" / "IncidentHJx" for this face: every
+     * injector on the face shares the first one's grid, and its extent. */
+    const int nl = isH ? s->nIH : s->nIE;
+    for (int q = 0; q < nl; ++q) {
+      const inc_layer *F = isH ? &s->IHlay[q] : &s->IElay[q];
+      if (F->dir == dir) { L->box = F->box; break; }
+    }
     L->off[L->dim] = isH ? (reverse ? +1 : 0) : -1;
     if (isH) s->nIH++; else s->nIE++;
   }
@@ -647,16 +655,19 @@ static void add_layer(mpo_sim *s, double **tot, const box3 *b, int comp[2], doub
 
 /* IncidentSourceECurrent::stepScheme (incsource.t:40-73) /
  * IncidentSourceHCurrent::stepScheme (incsource.t:112-145), written straight
- * into the totals. */
-static void inc_add(mpo_sim *s, inc_layer *L, double **tot) {
+ * into the totals.  Injectors on one face share one grid (add_inc_layers), so
+ * after all their stepScheme calls it holds the values of the last of them,
+ * and sumCurrents adds that grid once per injector: `writer` is the source
+ * whose values the shared grid holds. */
+static void inc_add(mpo_sim *s, inc_layer *L, int writer, double **tot) {
   const box3 *b = &L->box;
   for (int k = b->lo[2]; k <= b->hi[2]; ++k)
     for (int j = b->lo[1]; j <= b->hi[1]; ++j)
       for (int i = b->lo[0]; i <= b->hi[0]; ++i) {
         const int x = i + L->off[0], y = j + L->off[1], z = k + L->off[2];
         double f[3];
-        if (L->isH) src_efield(s, L->src, x, y, z, s->time, f);
-        else src_hfield(s, L->src, x, y, z, s->time, f);
+        if (L->isH) src_efield(s, writer, x, y, z, s->time, f);
+        else src_hfield(s, writer, x, y, z, s->time, f);
         const size_t g = IDX(s, i, j, k);
         tot[L->t1][g] += f[L->t2] / L->DX;
         tot[L->t2][g] += f[L->t1] / L->DX;
@@ -681,7 +692,15 @@ static void sum_currents(mpo_sim *s, int mag) {
     add_layer(s, tot, &L->box, comp, L->psi);
   }
   const int ni = mag ? s->nIH : s->nIE;
-  for (int l = 0; l < ni; ++l) inc_add(s, mag ? &s->IHlay[l] : &s->IElay[l], tot);
+  for (int l = 0; l < ni; ++l) {
+    inc_layer *L = mag ? &s->IHlay[l] : &s->IElay[l];
+    int writer = L->src;
+    for (int q = 0; q < ni; ++q) {
+      const inc_layer *F = mag ? &s->IHlay[q] : &s->IElay[q];
+      if (F->dir == L->dir) writer = F->src;
+    }
+    inc_add(s, L, writer, tot);
+  }
 }
 
 /* ------------------------------------------------------------------------ */

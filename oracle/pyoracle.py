@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "mpulse_ref")
 REF_BIN_FAST = os.path.join(HERE, "_ref", "mpulse_ref_fast")
+REF_BIN_GPU = os.path.join(HERE, "_ref", "mpulse_ref_gpu")
 
 _lib = None
 
@@ -133,13 +134,16 @@ def _fmt(x) -> str:
     return repr(float(x))
 
 
-def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None) -> str:
-    """MPulse setup file (rebuild.cpp grammar) describing `cfg`."""
+def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver_name: str | None = None,
+               extra: str = "") -> str:
+    """MPulse setup file (rebuild.cpp grammar) describing `cfg`.  `solver_name`
+    replaces the solver block's name (e.g. "fdtd-gpu-plrc-nonlin" for the B200
+    plug-in, which reads the same keys); `extra` is appended to its body."""
     g = (f"globals {{ grid-x {cfg.nx} grid-y {cfg.ny} grid-z {cfg.nz} "
          f"grid-dx {_fmt(cfg.dx)} grid-dy {_fmt(cfg.dy)} grid-dz {_fmt(cfg.dz)} "
          f"dt {_fmt(cfg.dt)} T-total {steps} }}\n")
     bnd = "single_periodic { }" if cfg.boundary == abi.MP_BOUNDARY_PERIODIC else "single_xy_periodic { }"
-    solver = _SOLVER_NAMES[cfg.solver]
+    solver = solver_name or _SOLVER_NAMES[cfg.solver]
     body = [f"eps {_fmt(cfg.eps)}"]
     if cfg.solver in (abi.MP_SOLVER_NL, abi.MP_SOLVER_PLRC_NONLIN):
         body.append(f"chi {_fmt(cfg.chi)}")
@@ -172,6 +176,8 @@ def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None) -> str
                     f"Phase {_fmt(s.phase)}", f"amp {_fmt(s.amp)}", f"eps {_fmt(s.eps)}"]) + " }")
             else:
                 raise ValueError(f"source kind {s.kind} has no runnable reference plug-in")
+    if extra:
+        body.append(extra)
     init = f"raw_init {{ file {init_file} }}\n" if init_file else ""
     return g + "fieldsim {\n  " + bnd + "\n  " + solver + " { " + " ".join(body) + " }\n  " + init + "}\n"
 
@@ -199,12 +205,14 @@ def full_to_plane(cfg: abi.Config, full: np.ndarray) -> np.ndarray:
 
 
 def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
-                  names=abi.FIELD_NAMES, binary: str = REF_BIN, workdir: str | None = None):
+                  names=abi.FIELD_NAMES, binary: str = REF_BIN, workdir: str | None = None,
+                  solver_name: str | None = None, extra: str = ""):
     """Runs the reference build for `steps` steps from the given initial fields
     (plane layout; missing components are zero) and returns
-    ({name: plane-layout array}, timing dict)."""
+    ({name: plane-layout array}, timing dict).  With binary=REF_BIN_GPU and a
+    "fdtd-gpu-*" solver_name, MPulse's own driver runs the B200 plug-in."""
     if not os.path.exists(binary):
-        raise RuntimeError(f"reference build missing: run `make -C {HERE} ref`")
+        raise RuntimeError(f"reference build missing: run `make -C {HERE} ref gpuref`")
     tmp = workdir or tempfile.mkdtemp(prefix="mpref_")
     init_path = None
     if init_fields:
@@ -217,7 +225,7 @@ def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
                 f.write(np.ascontiguousarray(full).tobytes())
     setup = os.path.join(tmp, "setup.dat")
     with open(setup, "w") as f:
-        f.write(setup_text(cfg, steps, init_path))
+        f.write(setup_text(cfg, steps, init_path, solver_name=solver_name, extra=extra))
     r = subprocess.run([binary, setup, tmp, *names], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"reference failed ({r.returncode}): {r.stderr[-2000:]}")

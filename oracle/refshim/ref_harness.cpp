@@ -46,6 +46,11 @@
 #undef private
 #undef protected
 
+#ifdef MPB_WITH_GPU
+// MPulse with the B200 FieldSolver plug-in registered beside its own solvers
+#include "fdtd_gpu.h"
+#endif
+
 namespace {
 
 template <class Base>
@@ -157,6 +162,9 @@ class HarnessFieldSim : public FieldSimulation {
         WParameter(new ParameterRebuild<MaskedNonlin, FieldSolver>(&solver));
     (*pm)["raw_init"] =
         WParameter(new ParameterRebuild<RawInit, FieldSimInit>(&initializers));
+#ifdef MPB_WITH_GPU
+    registerGpuSolvers(pm, &solver);
+#endif
     return pm;
   }
 };

@@ -229,6 +229,12 @@ int mp_sync(mp_ctx *ctx);
 int mp_device_field(mp_ctx *ctx, const char *name, void **dptr, size_t *count,
                     int *elem_bytes);
 
+/* Total field energy as FieldEnergyDiag::calculate (src/fielddiag.cpp:255-286)
+ * computes it: dx dy dz times the sum over the interior cells of
+ * Ex^2 + Ey^2 + Ez^2 + Bx^2 + By^2 + Bz^2, accumulated in FP64 whatever the
+ * field precision.  Synchronises the context's stream. */
+int mp_field_energy(mp_ctx *ctx, double *energy);
+
 /* Number of CUDA kernel launches the context has issued so far. */
 long long mp_launch_count(mp_ctx *ctx);
 

@@ -32,6 +32,8 @@ cudaError_t launch_convert_in(const double *src, void *dst, int fp32, long long 
                               cudaStream_t st);
 cudaError_t launch_convert_out(const void *src, double *dst, int fp32, long long n, int stride, int offset,
                                cudaStream_t st);
+cudaError_t launch_field_energy(const void *const fields[6], int elem_bytes, int nx, int ny, int nz, double dV,
+                                double *partial, double *out_dev, cudaStream_t st);
 }  // namespace mpb
 
 using namespace mpb;
@@ -80,6 +82,8 @@ struct mp_ctx {
   int *d_status = nullptr;
   int *h_status = nullptr;
   double *staging = nullptr;
+  double *d_diag = nullptr;   // diagnostics scratch: per-plane partials, then the result
+  double *h_diag = nullptr;   // pinned result
   size_t staging_n = 0;
   long long time = 0;
   long long launches = 0;
@@ -523,6 +527,8 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   }
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_status), ST_COUNT * sizeof(int)), "status allocation");
   MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_status), ST_COUNT * sizeof(int)), "pinned allocation");
+  MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_diag), size_t(g.nz + 3) * sizeof(double)), "diagnostics allocation");
+  MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_diag), sizeof(double)), "pinned allocation");
 
   if (c->fp32) build_params<float>(c, c->epf, c->bpf, ikE_off, ikH_off, bzy_off, coef, numer, denom);
   else build_params<double>(c, c->epd, c->bpd, ikE_off, ikH_off, bzy_off, coef, numer, denom);
@@ -703,6 +709,7 @@ void mp_destroy(mp_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->staging) cudaFree(c->staging);
   if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->h_diag) cudaFreeHost(c->h_diag);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -848,6 +855,25 @@ int mp_device_field(mp_ctx *c, const char *name, void **dptr, size_t *count, int
 }
 
 long long mp_launch_count(mp_ctx *c) { return c ? c->launches : -1; }
+
+
+
+int mp_field_energy(mp_ctx *c, double *energy) {
+  if (!c || !energy) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  const mp_config &g = c->cfg;
+  const void *f[6];
+  for (int q = 0; q < 6; ++q) f[q] = c->F[q];
+  double *result = c->d_diag + (g.nz + 2);
+  cudaError_t e = launch_field_energy(f, c->esz, g.nx, g.ny, g.nz, g.dx * g.dy * g.dz, c->d_diag, result, c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "energy kernels");
+  c->launches += 2;
+  e = cudaMemcpyAsync(c->h_diag, result, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "energy read");
+  *energy = *c->h_diag;
+  return MP_OK;
+}
 
 int mp_kernel_times(mp_ctx *c, int n_steps, double *e_ms, double *b_ms, double *s_ms) {
   if (!c || n_steps < 1 || !e_ms || !b_ms || !s_ms) return MP_ERR_INVALID;

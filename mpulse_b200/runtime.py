@@ -23,7 +23,7 @@ EXPORTED = (
     "mp_config_defaults", "mp_create", "mp_destroy", "mp_set_stream", "mp_field_size",
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
-    "mp_last_error", "mp_create_error", "mp_kernel_times",
+    "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
 )
 
 _lib = None
@@ -77,6 +77,8 @@ def lib():
     L.mp_last_error.restype = C.c_int
     L.mp_kernel_times.argtypes = [vp, C.c_int, dp, dp, dp]
     L.mp_kernel_times.restype = C.c_int
+    L.mp_field_energy.argtypes = [vp, dp]
+    L.mp_field_energy.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
@@ -177,6 +179,12 @@ class Simulation:
         e, b, s = C.c_double(), C.c_double(), C.c_double()
         self._check(lib().mp_kernel_times(self._h, int(n), C.byref(e), C.byref(b), C.byref(s)))
         return {"e_half_ms": e.value, "b_half_ms": b.value, "sources_ms": s.value}
+
+    def field_energy(self) -> float:
+        """FieldEnergyDiag::calculate (fielddiag.cpp:255-286) on the device state."""
+        e = C.c_double()
+        self._check(lib().mp_field_energy(self._h, C.byref(e)))
+        return e.value
 
     @property
     def launches(self) -> int:

@@ -1073,6 +1073,21 @@ int mpo_step(mpo_sim *s, int n_steps) {
 long long mpo_get_time(const mpo_sim *s) { return s->time; }
 void mpo_set_time(mpo_sim *s, long long t) { s->time = t; }
 
+/* FieldEnergyDiag::calculate (fielddiag.cpp:255-286): sum over the interior of
+ * E^2 + B^2 in MPulse's loop order (i slowest, k fastest), times dx dy dz. */
+double mpo_field_energy(const mpo_sim *s) {
+  double energy = 0;
+  for (int i = 1; i <= s->cfg.nx; ++i)
+    for (int j = 1; j <= s->cfg.ny; ++j)
+      for (int k = 1; k <= s->cfg.nz; ++k) {
+        const size_t g = IDX(s, i, j, k);
+        const double ex = s->F[0][g], ey = s->F[1][g], ez = s->F[2][g];
+        const double bx = s->F[3][g], by = s->F[4][g], bz = s->F[5][g];
+        energy += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
+      }
+  return energy * (s->cfg.dx * s->cfg.dy * s->cfg.dz);
+}
+
 /* The Faddeeva evaluator on its own, for tests against scipy / the reference. */
 void mpo_faddeeva(const double *re, const double *im, double *wre, double *wim, size_t n) {
   oracle_faddeeva_init();

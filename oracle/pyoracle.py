@@ -50,6 +50,8 @@ def lib():
         L.mpo_source_field.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_longlong, C.POINTER(C.c_double)]
         L.mpo_source_field.restype = C.c_int
+        L.mpo_field_energy.argtypes = [C.c_void_p]
+        L.mpo_field_energy.restype = C.c_double
         _lib = L
     return _lib
 
@@ -100,6 +102,9 @@ class OracleSim:
     @time.setter
     def time(self, t: int):
         lib().mpo_set_time(self.h, t)
+
+    def field_energy(self) -> float:
+        return lib().mpo_field_energy(self.h)
 
     def source_field(self, src: int, which: int, i: int, j: int, l: int, time: int):
         out = np.zeros(3)

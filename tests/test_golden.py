@@ -45,3 +45,18 @@ def test_oracle_reproduces_reference_workload(path):
         assert np.linalg.norm(full[n][:, j, :] - d[n]) <= 1e-13 * total, n
     energy = sum(np.sum(full[n][1:-1] ** 2) for n in abi.FIELD_NAMES)
     assert abs(energy - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+
+
+def test_oracle_energy_matches_reference_diagnostic():
+    """mpo_field_energy restates FieldEnergyDiag::calculate; the workload
+    fixtures hold the reference's sum(E^2 + B^2) over the interior."""
+    for path in workload_files():
+        d, cfg = load(path)
+        init = workload_init(path, cfg)
+        o = pyoracle.OracleSim(cfg)
+        if init:
+            for n, v in init.items():
+                o.upload(n, v)
+        o.step(int(d["steps"]))
+        e = o.field_energy() / (cfg.dx * cfg.dy * cfg.dz)
+        assert abs(e - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))

@@ -111,3 +111,23 @@ def test_time_counter_and_sources_follow_process_time():
         assert g.time == 50
         for n in abi.FIELD_NAMES:
             assert rel_l2(g.download(n), o.download(n)) <= TOL_FP64
+
+
+@pytest.mark.parametrize("precision,tol", [(abi.MP_FP64, 1e-13), (abi.MP_FP32, 1e-5)])
+def test_field_energy_matches_oracle(precision, tol):
+    """mp_field_energy against the oracle's restatement of
+    FieldEnergyDiag::calculate (fielddiag.cpp:255-286)."""
+    cfg = make_case("nonlin_odd_sizes", precision)
+    cfg64 = make_case("nonlin_odd_sizes", abi.MP_FP64)
+    init = random_fields(cfg64, seed=31, smooth=True)
+    o = pyoracle.OracleSim(cfg64)
+    for n, v in init.items():
+        o.upload(n, v)
+    o.step(7)
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.step(7)
+        e = g.field_energy()
+    ref = o.field_energy()
+    assert abs(e - ref) <= tol * abs(ref)

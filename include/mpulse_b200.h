@@ -235,6 +235,41 @@ int mp_device_field(mp_ctx *ctx, const char *name, void **dptr, size_t *count,
  * field precision.  Synchronises the context's stream. */
 int mp_field_energy(mp_ctx *ctx, double *energy);
 
+/* Largest nz that mp_field_energy_noalloc accepts. */
+#define MP_NOALLOC_MAX_PLANES 16384
+
+/* The field energy of mp_field_energy for callers that cannot allocate device
+ * memory.  No counterpart in MPulse.
+ *
+ * Who needs it: code that owns all of its device memory itself - an
+ * application that runs its own pool or allocator and hands this library only
+ * pointers into it, a process held to a fixed device-memory budget, or a
+ * caller that must not enter cudaMalloc / cudaFree (they can synchronise the
+ * whole device and stall work queued by others).  Such a caller cannot create
+ * an mp_ctx (mp_create allocates) and so cannot use mp_field_energy, whose
+ * scratch lives in the context.
+ *
+ * What it does: the same two kernels as mp_field_energy on caller-owned
+ * device arrays.  fields[0..5] are Ex Ey Ez Bx By Bz in the plane layout
+ * above ((nz+2) * ny * nx elements each, elem_bytes 4 for FP32 or 8 for FP64);
+ * the interior planes 1..nz are summed, times dx dy dz, in FP64.  Work goes to
+ * cuda_stream (NULL: the legacy default stream); the call waits for it and
+ * writes the result to the host double *energy.
+ *
+ * Limit: the scratch is a fixed array compiled into the library
+ * (MP_NOALLOC_MAX_PLANES + 32 doubles, about 130 KB, held by every GPU that
+ * loads the library until the process exits), one partial sum per z-plane, so
+ * nz above MP_NOALLOC_MAX_PLANES is rejected with MP_ERR_INVALID and a message
+ * from mp_last_error(NULL, ..).  It allocates nothing: no cudaMalloc, no
+ * cudaFree, no allocating library call.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) once for that device;
+ * make that first call before any stream capture.  All calls share the array
+ * and it keeps the last call's contents (nothing in it needs to start at
+ * zero); calls whose work overlaps on the GPU race on it and must be
+ * serialised by the caller. */
+int mp_field_energy_noalloc(const void *const fields[6], int elem_bytes, int nx, int ny, int nz,
+                            double dx, double dy, double dz, void *cuda_stream, double *energy);
+
 /* Number of CUDA kernel launches the context has issued so far. */
 long long mp_launch_count(mp_ctx *ctx);
 

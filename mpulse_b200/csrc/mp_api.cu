@@ -856,7 +856,13 @@ int mp_device_field(mp_ctx *c, const char *name, void **dptr, size_t *count, int
 
 long long mp_launch_count(mp_ctx *c) { return c ? c->launches : -1; }
 
+}  // extern "C"
 
+namespace mpb {
+void set_global_error(const char *msg) { snprintf(g_create_err, sizeof g_create_err, "%s", msg); }
+}  // namespace mpb
+
+extern "C" {
 
 int mp_field_energy(mp_ctx *c, double *energy) {
   if (!c || !energy) return MP_ERR_INVALID;

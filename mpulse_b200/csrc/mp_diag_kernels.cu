@@ -6,13 +6,16 @@
 // Two passes, both deterministic: one block per z-plane sums that plane into a
 // per-plane partial (fixed tree order), then one block sums the partials in
 // plane order.  The per-plane partials are scratch memory: mp_field_energy uses
-// a buffer the context allocated.
+// a buffer the context allocated; mp_field_energy_noalloc uses the file-scope
+// array below instead.
 #include "mpulse_b200.h"
 
 #include "mp_device.h"
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <mutex>
 
 namespace mpb {
 
@@ -82,4 +85,89 @@ cudaError_t launch_field_energy(const void *const fields[6], int elem_bytes, int
   return cudaGetLastError();
 }
 
+void set_global_error(const char *msg);  // mp_api.cu: message for mp_last_error(NULL, ..)
+
 }  // namespace mpb
+
+// ---------------------------------------------------------------------------
+// mp_field_energy without allocating.
+//
+// The scratch of the two passes (one partial sum per z-plane, then the result)
+// lives in this fixed file-scope array instead of a context buffer.  It holds
+// MP_NOALLOC_MAX_PLANES partials plus the result slot (about 130 KB); every GPU
+// that loads the library keeps it until the process exits.  All calls on a
+// device share it and it keeps the last call's contents; nothing in it has to
+// start at zero, because a call writes every slot it reads before reading it.
+// Two calls whose work overlaps on the GPU (different streams, or different
+// host threads) race on it.
+static __device__ __align__(256) double g_energy_scratch[MP_NOALLOC_MAX_PLANES + 32];
+
+namespace {
+
+const int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double *g_scratch_addr[kMaxDevices];  // device address of g_energy_scratch, per device
+
+// The host-side name g_energy_scratch is a stand-in, not a device address;
+// the address comes from cudaGetSymbolAddress with the device current.
+cudaError_t scratch_for_current_device(double **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_energy_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[dev] = static_cast<double *>(p);
+  }
+  *out = g_scratch_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int mp_field_energy_noalloc(const void *const fields[6], int elem_bytes, int nx, int ny, int nz,
+                                       double dx, double dy, double dz, void *cuda_stream, double *energy) {
+  char msg[256];
+  if (!fields || !energy) {
+    mpb::set_global_error("mp_field_energy_noalloc: fields and energy must not be NULL");
+    return MP_ERR_INVALID;
+  }
+  for (int c = 0; c < 6; ++c)
+    if (!fields[c]) {
+      mpb::set_global_error("mp_field_energy_noalloc: a field pointer is NULL");
+      return MP_ERR_INVALID;
+    }
+  if (elem_bytes != 4 && elem_bytes != 8) {
+    mpb::set_global_error("mp_field_energy_noalloc: elem_bytes must be 4 (FP32) or 8 (FP64)");
+    return MP_ERR_INVALID;
+  }
+  if (nx < 1 || ny < 1 || nz < 1) {
+    mpb::set_global_error("mp_field_energy_noalloc: nx, ny, nz must be positive");
+    return MP_ERR_INVALID;
+  }
+  if (nz > MP_NOALLOC_MAX_PLANES) {
+    snprintf(msg, sizeof msg,
+             "mp_field_energy_noalloc: nz = %d exceeds the %d planes of its fixed scratch array; "
+             "use mp_field_energy", nz, MP_NOALLOC_MAX_PLANES);
+    mpb::set_global_error(msg);
+    return MP_ERR_INVALID;
+  }
+  double *scratch = nullptr;
+  cudaError_t e = scratch_for_current_device(&scratch);
+  if (e == cudaSuccess) {
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    double *result = scratch + MP_NOALLOC_MAX_PLANES;
+    e = mpb::launch_field_energy(fields, elem_bytes, nx, ny, nz, dx * dy * dz, scratch, result, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(energy, result, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (e != cudaSuccess) {
+    snprintf(msg, sizeof msg, "mp_field_energy_noalloc: %s", cudaGetErrorString(e));
+    mpb::set_global_error(msg);
+    return MP_ERR_CUDA;
+  }
+  return MP_OK;
+}

@@ -24,6 +24,7 @@ EXPORTED = (
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
+    "mp_field_energy_noalloc",
 )
 
 _lib = None
@@ -79,6 +80,9 @@ def lib():
     L.mp_kernel_times.restype = C.c_int
     L.mp_field_energy.argtypes = [vp, dp]
     L.mp_field_energy.restype = C.c_int
+    L.mp_field_energy_noalloc.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, vp, dp]
+    L.mp_field_energy_noalloc.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L

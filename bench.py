@@ -277,9 +277,10 @@ def run_profile(args) -> dict:
     sim.step(args.warmup)
     dt, launches = time_steps(sim, torch, args.steps, stream)
     cells = cfg.nx * cfg.ny * cfg.nz
+    kt = sim.kernel_times(5)
     sim.close()
     return {"profile_run": True, "grid": [cfg.nx, cfg.ny, cfg.nz], "steps": args.steps,
-            "value": cells * args.steps / dt / 1e9, "unit": UNIT, "gpu_launches": launches}
+            "value": cells * args.steps / dt / 1e9, "unit": UNIT, "gpu_launches": launches, "kernel_ms": kt}
 
 
 def run_e2e(args, torch, stream, local_rank) -> dict:

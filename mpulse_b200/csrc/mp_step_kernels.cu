@@ -23,6 +23,17 @@
 
 #include <cuda_runtime.h>
 
+// Minimum resident blocks per SM asked of the register allocator.  Measured
+// on the 256x256x512 PLRC + Kerr workload (FP32): E half 1.083 ms with no
+// bound (114 registers), 0.917 ms with 3 blocks (80 registers, 28 B spilled),
+// 1.17 ms with 4 (64 registers, more spills); the B half does not move.
+#ifndef MPB_E_MIN_BLOCKS
+#define MPB_E_MIN_BLOCKS 3
+#endif
+#ifndef MPB_B_MIN_BLOCKS
+#define MPB_B_MIN_BLOCKS 1
+#endif
+
 namespace mpb {
 
 template <typename T> struct Vec2;
@@ -66,7 +77,7 @@ __device__ __forceinline__ double nl_newton(double E, double eps, double chi, do
 }
 
 template <typename T, int MODE, int NP>
-__global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
+__global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EParams<T> p) {
   typedef typename Vec2<T>::type T2;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based: MPulse i + 1
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -261,7 +272,7 @@ __global__ void __launch_bounds__(256) e_half_kernel(const EParams<T> p) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) b_half_kernel(const BParams<T> p) {
+__global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BParams<T> p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.nx || j >= p.ny) return;

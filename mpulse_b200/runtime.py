@@ -16,7 +16,8 @@ import numpy as np
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmpulse_b200.so")
+# MPULSE_B200_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("MPULSE_B200_LIB") or os.path.join(HERE, "libmpulse_b200.so")
 
 # Every entry point include/mpulse_b200.h declares.
 EXPORTED = (

@@ -102,8 +102,16 @@ typedef enum mp_source_kind {
   MP_SOURCE_PLANE_WAVE = 1,     /* "wave_inject"        sources.cpp:8-173 */
   MP_SOURCE_PLANE_GAUSS = 2,    /* "plane_gauss_inject" sources.cpp:179-331 */
   MP_SOURCE_SHORT_PULSE = 3,    /* "short_pulse_inject" shortpulseinject.cpp */
-  MP_SOURCE_FOCUSED_PULSE = 4   /* "focused_pulse_inject" (see mp_source) */
+  MP_SOURCE_FOCUSED_PULSE = 4,  /* "focused_pulse_inject" (see mp_source) */
+  MP_SOURCE_GAUSS_BEAM = 5      /* "gauss_inject"       gaussinject.cpp */
 } mp_source_kind;
+
+/* Kernel form of the step; all forms give bit-identical results.  GLOBAL reads
+ * global memory directly (L1/L2 serve the neighbours); TMA stages each z-plane
+ * in a shared-memory ring with TMA tile loads (needs nx a multiple of 32 and
+ * ny of 8, else mp_create fails with MP_ERR_UNSUPPORTED); AUTO picks the form
+ * measured fastest on B200, currently GLOBAL. */
+typedef enum mp_staging { MP_STAGING_AUTO = 0, MP_STAGING_GLOBAL = 1, MP_STAGING_TMA = 2 } mp_staging;
 
 /* One Lorentz pole: MPulse's L<n>eps, L<n>delta, L<n>Om2
  * (src/fdtd_plrc.t:419-429, src/fdtd_plrc.h:85-90). */
@@ -133,7 +141,13 @@ typedef struct mp_source {
   double t_shift;    /* TShift */
   double z_shift;    /* ZShift (focus offset from the grid centre) */
   double phase;      /* Phase, in units of 2 pi */
-  double amp;        /* peak amplitude of Re Ex at the focus */
+  double amp;        /* short pulse: peak Re Ex at the focus; gauss_inject: amp */
+  /* gauss_inject (gaussinject.cpp:33-48); also uses length, width, amp, eps */
+  int t_size;        /* SizeT: samples of the time transform (default 4096) */
+  int t_off;         /* toff: first step of the injection (default 0) */
+  double k0;         /* k0: central wavenumber (default 2 pi) */
+  double shift;      /* Shift: focal shift along z */
+  double time;       /* Time: time shift of the spectrum */
 } mp_source;
 
 typedef struct mp_config {
@@ -172,6 +186,7 @@ typedef struct mp_config {
   int newton_max_iter;      /* default 64 */
   double newton_tol;        /* default 1e-9 */
 
+  int staging;              /* mp_staging: kernel form (results are the same) */
   int device;               /* CUDA device ordinal */
 } mp_config;
 

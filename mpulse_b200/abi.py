@@ -37,8 +37,9 @@ MP_FP64, MP_FP32 = 0, 1
 MP_SOLVER_PLAIN, MP_SOLVER_NL, MP_SOLVER_PLRC_LIN, MP_SOLVER_PLRC_NONLIN = 0, 1, 2, 3
 MP_BOUNDARY_PERIODIC, MP_BOUNDARY_XY_PERIODIC = 0, 1
 MP_CPML_NONE, MP_CPML_ALL, MP_CPML_Z = 0, 1, 2
+MP_STAGING_AUTO, MP_STAGING_GLOBAL, MP_STAGING_TMA = 0, 1, 2
 (MP_SOURCE_NONE, MP_SOURCE_PLANE_WAVE, MP_SOURCE_PLANE_GAUSS,
- MP_SOURCE_SHORT_PULSE, MP_SOURCE_FOCUSED_PULSE) = range(5)
+ MP_SOURCE_SHORT_PULSE, MP_SOURCE_FOCUSED_PULSE, MP_SOURCE_GAUSS_BEAM) = range(6)
 
 FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz")
 PSI_NAMES = tuple(f"Psi{ri}{n}{c}" for ri in "RI" for n in (1, 2, 3) for c in "xyz")
@@ -67,6 +68,11 @@ class Source(C.Structure):
         ("z_shift", C.c_double),
         ("phase", C.c_double),
         ("amp", C.c_double),
+        ("t_size", C.c_int),
+        ("t_off", C.c_int),
+        ("k0", C.c_double),
+        ("shift", C.c_double),
+        ("time", C.c_double),
     ]
 
 
@@ -98,6 +104,7 @@ class Config(C.Structure):
         ("sources", Source * MP_MAX_SOURCES),
         ("newton_max_iter", C.c_int),
         ("newton_tol", C.c_double),
+        ("staging", C.c_int),
         ("device", C.c_int),
     ]
 
@@ -125,6 +132,9 @@ def default_source(kind: int = MP_SOURCE_NONE) -> Source:
     s.waist = 1.0
     s.om0 = 2 * math.pi
     s.amp = 1.0
+    s.t_size = 4096
+    s.t_off = 0
+    s.k0 = 2 * math.pi
     return s
 
 
@@ -159,6 +169,7 @@ def default_config() -> Config:
         c.sources[n] = default_source()
     c.newton_max_iter = 64
     c.newton_tol = 1e-9
+    c.staging = MP_STAGING_AUTO
     c.device = 0
     return c
 

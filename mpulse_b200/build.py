@@ -22,6 +22,9 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libmpulse_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# cuFFT: the once-per-block spectral precompute of gauss_inject
+CUDA_LIB = "/usr/local/cuda/lib64"
+LINK_LIBS = ["-L" + CUDA_LIB, "-lcufft", "-Xlinker", "-rpath=" + CUDA_LIB]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-I" + INCLUDE, "-I" + CSRC]
 
@@ -53,7 +56,7 @@ def build(verbose: bool = False) -> str:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if _newer(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", *LINK_LIBS]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -11,6 +11,7 @@
 #include "mpulse_b200.h"
 
 #include "mp_device.h"
+#include "mp_gauss.h"
 #include "mp_pulse_math.h"
 
 #include <cuda_runtime.h>
@@ -27,13 +28,19 @@
 namespace mpb {
 template <typename T> cudaError_t launch_e_half(const EParams<T> &, int, int, cudaStream_t);
 template <typename T> cudaError_t launch_b_half(const BParams<T> &, cudaStream_t);
-template <typename T> cudaError_t launch_source_plane(const SourceEvalParams &, T *, T *, cudaStream_t);
+template <typename T>
+cudaError_t launch_source_batch(const SourceEvalParams &, const SourceEvalParams &, long long, int, T *, cudaStream_t);
 cudaError_t launch_convert_in(const double *src, void *dst, int fp32, long long n, int stride, int offset,
                               cudaStream_t st);
 cudaError_t launch_convert_out(const void *src, double *dst, int fp32, long long n, int stride, int offset,
                                cudaStream_t st);
 cudaError_t launch_field_energy(const void *const fields[6], int elem_bytes, int nx, int ny, int nz, double dV,
                                 double *partial, double *out_dev, cudaStream_t st);
+template <typename T>
+cudaError_t launch_e_half_tma(const EParams<T> &, const ETmaMaps &, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_b_half_tma(const BParams<T> &, const BTmaMaps &, cudaStream_t);
+void tma_boxes(int esz, int e_box[7][2], int b_box[6][2]);
 }  // namespace mpb
 
 using namespace mpb;
@@ -77,7 +84,9 @@ struct mp_ctx {
   int src_mult = 0;
   SourceEvalParams sq[MP_MAX_SOURCES][2];
   int src_plane[MP_MAX_SOURCES][2];
-  void *src_buf = nullptr;
+  void *src_buf = nullptr;   // injection planes of up to src_batch steps
+  int src_batch = 1;
+  GaussBeam *gauss = nullptr;  // gauss_inject state when the last injector is one
   double *d_wcoef = nullptr;
   int *d_status = nullptr;
   int *h_status = nullptr;
@@ -93,6 +102,9 @@ struct mp_ctx {
   BParams<float> bpf;
   EParams<double> epd;
   BParams<double> bpd;
+  bool tma = false;  // TMA-staged kernels in use
+  ETmaMaps etma;
+  BTmaMaps btma;
   std::vector<void *> allocs;
 };
 
@@ -188,13 +200,20 @@ int validate(const mp_config *c) {
     const mp_source &q = c->sources[s];
     if (q.kind == MP_SOURCE_FOCUSED_PULSE)
       return set_err(nullptr, MP_ERR_UNSUPPORTED, "focused_pulse_inject is not built");
-    if (q.kind < MP_SOURCE_PLANE_WAVE || q.kind > MP_SOURCE_SHORT_PULSE)
+    if (q.kind < MP_SOURCE_PLANE_WAVE || q.kind > MP_SOURCE_GAUSS_BEAM)
       return set_err(nullptr, MP_ERR_INVALID, "source %d: unknown kind %d", s, q.kind);
+    if (q.kind == MP_SOURCE_GAUSS_BEAM && (q.t_size < 1 || q.t_size > (1 << 22)))
+      return set_err(nullptr, MP_ERR_INVALID, "source %d: t_size %d outside 1..2^22", s, q.t_size);
     if (q.distance < 1 || q.distance > c->nz)
       return set_err(nullptr, MP_ERR_INVALID, "source %d: distance %d outside 1..nz", s, q.distance);
     if (!(q.eps > 0)) return set_err(nullptr, MP_ERR_INVALID, "source %d: eps must be positive", s);
   }
   if (c->newton_max_iter < 1) return set_err(nullptr, MP_ERR_INVALID, "newton_max_iter must be >= 1");
+  if (c->staging != MP_STAGING_AUTO && c->staging != MP_STAGING_GLOBAL && c->staging != MP_STAGING_TMA)
+    return set_err(nullptr, MP_ERR_INVALID, "unknown staging %d", c->staging);
+  if (c->staging == MP_STAGING_TMA && (c->nx % kTmaTileX != 0 || c->ny % kTmaTileY != 0))
+    return set_err(nullptr, MP_ERR_UNSUPPORTED, "TMA staging needs nx a multiple of %d and ny of %d", kTmaTileX,
+                   kTmaTileY);
   return MP_OK;
 }
 
@@ -278,6 +297,7 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
     bp.src[s].v1 = base + 3 * pl;
   }
   ep.status = c->d_status;
+  bp.status = c->d_status;
   // planes per block: enough blocks to fill 148 SMs several times over
   const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
   const long long target = 148LL * 8;
@@ -285,6 +305,64 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
   const long long chunks = std::max(1LL, (target + blocks_xy - 1) / blocks_xy);
   ep.kchunk = int(std::max(1LL, (ne + chunks - 1) / chunks));
   bp.kchunk = int(std::max(1LL, (nb + chunks - 1) / chunks));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 3-D map over an array of `dz` planes of dy rows of dx elements, box bx x by x 1.
+bool encode_map(CUtensorMap *m, void *base, int esz, long long dx, long long dy, long long dz, int bx, int by) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || !base) return false;
+  const cuuint64_t dims[3] = {cuuint64_t(dx), cuuint64_t(dy), cuuint64_t(dz)};
+  const cuuint64_t strides[2] = {cuuint64_t(dx * esz), cuuint64_t(dx * dy * esz)};
+  const cuuint32_t box[3] = {cuuint32_t(bx), cuuint32_t(by), 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides,
+            box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of the TMA-staged kernels; false (global-load kernels are used)
+// if the driver cannot encode them.
+bool setup_tma(mp_ctx *c) {
+  const mp_config &g = c->cfg;
+  int eb[7][2], bb[6][2];
+  tma_boxes(c->esz, eb, bb);
+  const long long nx = g.nx, ny = g.ny, nzp = g.nz + 2;
+  bool ok = true;
+  ok = ok && encode_map(&c->etma.bx, c->F[3], c->esz, nx, ny, nzp, eb[0][0], eb[0][1]);
+  ok = ok && encode_map(&c->etma.by, c->F[4], c->esz, nx, ny, nzp, eb[1][0], eb[1][1]);
+  ok = ok && encode_map(&c->etma.bz, c->F[5], c->esz, nx, ny, nzp, eb[2][0], eb[2][1]);
+  ok = ok && encode_map(&c->etma.ex, c->F[0], c->esz, nx, ny, nzp, eb[3][0], eb[3][1]);
+  ok = ok && encode_map(&c->etma.ey, c->F[1], c->esz, nx, ny, nzp, eb[4][0], eb[4][1]);
+  ok = ok && encode_map(&c->etma.ez, c->F[2], c->esz, nx, ny, nzp, eb[5][0], eb[5][1]);
+  for (int s = 0; s < c->np && ok; ++s)
+    for (int a = 0; a < 3 && ok; ++a)
+      ok = encode_map(&c->etma.psi[s][a], c->psi[s][a], c->esz, 2 * nx, ny, c->mz1 - c->mz0 + 1, eb[6][0], eb[6][1]);
+  ok = ok && encode_map(&c->btma.ex, c->F[0], c->esz, nx, ny, nzp, bb[0][0], bb[0][1]);
+  ok = ok && encode_map(&c->btma.ey, c->F[1], c->esz, nx, ny, nzp, bb[1][0], bb[1][1]);
+  ok = ok && encode_map(&c->btma.ez, c->F[2], c->esz, nx, ny, nzp, bb[2][0], bb[2][1]);
+  ok = ok && encode_map(&c->btma.bx, c->F[3], c->esz, nx, ny, nzp, bb[3][0], bb[3][1]);
+  ok = ok && encode_map(&c->btma.by, c->F[4], c->esz, nx, ny, nzp, bb[4][0], bb[4][1]);
+  ok = ok && encode_map(&c->btma.bz, c->F[5], c->esz, nx, ny, nzp, bb[5][0], bb[5][1]);
+  c->tma = ok;
+  return ok;
 }
 
 int create_impl(const mp_config *cfg, mp_ctx **out) {
@@ -488,6 +566,10 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
         p.ramp = q.ramp;
         p.width = q.width;
         p.offset = q.offset;
+      } else if (q.kind == MP_SOURCE_GAUSS_BEAM) {
+        // getHField scales Bx by sqrt(eps) amp, getEField Ex / Ey by amp
+        // (gaussinject.cpp:204-222); the planes are set per block in step_impl
+        p.g_scale = isH ? q.amp : std::sqrt(q.eps) * q.amp;
       } else {
         // ShortPulseInjectSourceFunc::setParam (shortpulseinject.cpp:56-113)
         p.centre[0] = 0.5 * double(g.nx + 1);
@@ -511,8 +593,26 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
     }
     c->src_plane[s][0] = first.distance;      // E current layer z = d
     c->src_plane[s][1] = first.distance - 1;  // H current layer z = d - 1 (incsource.t:91)
+    if (q.kind == MP_SOURCE_GAUSS_BEAM) {
+      c->gauss = new (std::nothrow) GaussBeam();
+      if (!c->gauss) return fail(set_err(c, MP_ERR_NO_MEMORY, "gauss_inject state"));
+      const int grc = gauss_create(*c->gauss, q, g, &c->err);
+      if (grc != MP_OK) {
+        delete c->gauss;
+        c->gauss = nullptr;
+        return fail(grc);
+      }
+      c->sq[s][0].g_f1 = c->gauss->bx;
+      c->sq[s][1].g_f1 = c->gauss->ex;
+      c->sq[s][1].g_f2 = c->gauss->ey;
+    }
   }
-  if (c->nsrc) MPB_TRY(dalloc(c, &c->src_buf, size_t(c->nsrc) * 4 * size_t(c->plane) * c->esz), "source allocation");
+  if (c->nsrc) {
+    // plane pairs for up to 64 steps ahead, at most 256 MB
+    const size_t per_step = 4 * size_t(c->plane) * c->esz;
+    c->src_batch = int(std::max<size_t>(1, std::min<size_t>(64, (size_t(256) << 20) / per_step)));
+    MPB_TRY(dalloc(c, &c->src_buf, size_t(c->src_batch) * per_step), "source allocation");
+  }
 
   // upload the lines
   MPB_TRY(dalloc(c, &c->lines, host_lines.size() * c->esz), "line allocation");
@@ -532,6 +632,21 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
 
   if (c->fp32) build_params<float>(c, c->epf, c->bpf, ikE_off, ikH_off, bzy_off, coef, numer, denom);
   else build_params<double>(c, c->epd, c->bpd, ikE_off, ikH_off, bzy_off, coef, numer, denom);
+  // AUTO = GLOBAL: on the 256x256x512 PLRC + Kerr workload the global-load
+  // kernels (E 0.92 ms, B 0.47 ms per launch) beat the TMA-staged ones
+  // (E 1.12 ms, B 0.61 ms), whose 12 small tile copies per plane and block
+  // serialise in the copy engine.
+  if (g.staging == MP_STAGING_TMA) {
+    if (!setup_tma(c)) return fail(set_err(c, MP_ERR_UNSUPPORTED, "TMA tensor maps could not be encoded"));
+    // TMA kernels: two resident blocks per SM; about four waves of blocks so
+    // each block's pipeline runs over a long chunk of planes
+    const long long tiles = (long long)(g.nx / kTmaTileX) * (g.ny / kTmaTileY);
+    const long long chunks = std::max(1LL, (148LL * 8 + tiles - 1) / tiles);
+    const int ne = g.nz + 2, nb = g.nz + 2;
+    const int ke = int(std::max(1LL, (ne + chunks - 1) / chunks)), kb = int(std::max(1LL, (nb + chunks - 1) / chunks));
+    if (c->fp32) { c->epf.kchunk = ke; c->bpf.kchunk = kb; }
+    else { c->epd.kchunk = ke; c->bpd.kchunk = kb; }
+  }
   MPB_TRY(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
 #undef MPB_TRY
   *out = c;
@@ -600,46 +715,74 @@ struct StepTimer {
   bool on = false;
 };
 
+// Per step: E half, B half.  The injection planes of a block of up to
+// src_batch steps are computed ahead in one launch (they depend on
+// Process::time only), and each half step reads its step's plane pair.
 template <typename T>
 int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer *tm = nullptr,
               double *acc = nullptr) {
-  for (int t = 0; t < n_steps; ++t) {
+  const size_t pl = size_t(c->plane);
+  int t = 0;
+  while (t < n_steps) {
+    int K = c->nsrc ? std::min(c->src_batch, n_steps - t) : n_steps - t;
     cudaError_t e;
-    if (tm) cudaEventRecord(tm->ev[0], c->stream);
-    for (int s = 0; s < c->nsrc; ++s) {
-      c->sq[s][0].time = c->time;
-      T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * size_t(c->plane);
-      e = launch_source_plane<T>(c->sq[s][0], base, base + c->plane, c->stream);
+    if (c->nsrc) {
+      if (tm) cudaEventRecord(tm->ev[4], c->stream);
+      if (c->gauss) {
+        // the block holding this step (computed here when it changes); the
+        // batch ends where the source's state changes next
+        bool active;
+        long long toff, until;
+        const int rc = gauss_prepare(*c->gauss, c->time, c->stream, &active, &toff, &until, &c->launches, &c->err);
+        if (rc != MP_OK) return rc;
+        if (until > c->time) K = int(std::min<long long>(K, until - c->time));
+        for (int side = 0; side < 2; ++side) {
+          c->sq[0][side].g_active = active ? 1 : 0;
+          c->sq[0][side].g_toff = toff;
+        }
+      }
+      e = launch_source_batch<T>(c->sq[0][0], c->sq[0][1], c->time, K, static_cast<T *>(c->src_buf), c->stream);
       if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
       c->launches++;
+      if (tm) {
+        cudaEventRecord(tm->ev[5], c->stream);
+        e = cudaEventSynchronize(tm->ev[5]);
+        if (e != cudaSuccess) return cuda_err(c, e, "event synchronize");
+        float ms;
+        cudaEventElapsedTime(&ms, tm->ev[4], tm->ev[5]);
+        acc[2] += ms;  // sources, all steps of the block
+      }
     }
-    if (tm) cudaEventRecord(tm->ev[1], c->stream);
-    e = launch_e_half<T>(ep, c->mode, c->np, c->stream);
-    if (e != cudaSuccess) return cuda_err(c, e, "E half-step kernel");
-    c->launches++;
-    if (tm) cudaEventRecord(tm->ev[2], c->stream);
-    for (int s = 0; s < c->nsrc; ++s) {
-      c->sq[s][1].time = c->time;
-      T *base = static_cast<T *>(c->src_buf) + size_t(s) * 4 * size_t(c->plane);
-      e = launch_source_plane<T>(c->sq[s][1], base + 2 * c->plane, base + 3 * c->plane, c->stream);
-      if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
+    for (int q = 0; q < K; ++q) {
+      if (c->nsrc) {
+        const T *base = static_cast<const T *>(c->src_buf) + size_t(q) * 4 * pl;
+        ep.src[0].v0 = base;
+        ep.src[0].v1 = base + pl;
+        bp.src[0].v0 = base + 2 * pl;
+        bp.src[0].v1 = base + 3 * pl;
+      }
+      if (tm) cudaEventRecord(tm->ev[0], c->stream);
+      e = c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
+                 : launch_e_half<T>(ep, c->mode, c->np, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "E half-step kernel");
       c->launches++;
+      if (tm) cudaEventRecord(tm->ev[1], c->stream);
+      e = c->tma ? launch_b_half_tma<T>(bp, c->btma, c->stream) : launch_b_half<T>(bp, c->stream);
+      if (e != cudaSuccess) return cuda_err(c, e, "B half-step kernel");
+      c->launches++;
+      if (tm) {
+        cudaEventRecord(tm->ev[2], c->stream);
+        e = cudaEventSynchronize(tm->ev[2]);
+        if (e != cudaSuccess) return cuda_err(c, e, "event synchronize");
+        float ms[2];
+        cudaEventElapsedTime(&ms[0], tm->ev[0], tm->ev[1]);
+        cudaEventElapsedTime(&ms[1], tm->ev[1], tm->ev[2]);
+        acc[0] += ms[0];  // E half
+        acc[1] += ms[1];  // B half
+      }
+      c->time++;
     }
-    if (tm) cudaEventRecord(tm->ev[3], c->stream);
-    e = launch_b_half<T>(bp, c->stream);
-    if (e != cudaSuccess) return cuda_err(c, e, "B half-step kernel");
-    c->launches++;
-    if (tm) {
-      cudaEventRecord(tm->ev[4], c->stream);
-      e = cudaEventSynchronize(tm->ev[4]);
-      if (e != cudaSuccess) return cuda_err(c, e, "event synchronize");
-      float ms[4];
-      for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&ms[q], tm->ev[q], tm->ev[q + 1]);
-      acc[0] += ms[1];          // E half
-      acc[1] += ms[3];          // B half
-      acc[2] += ms[0] + ms[2];  // sources
-    }
-    c->time++;
+    t += K;
   }
   return MP_OK;
 }
@@ -687,6 +830,9 @@ void mp_config_defaults(mp_config *c) {
     q.waist = 1.0;
     q.om0 = 2 * M_PI;
     q.amp = 1.0;
+    q.t_size = 4096;          // gaussinject.cpp:38-47
+    q.t_off = 0;
+    q.k0 = 2 * M_PI;
   }
   c->newton_max_iter = 64;
   c->newton_tol = 1e-9;       // fdtd_plrc.cpp:414
@@ -707,6 +853,10 @@ void mp_destroy(mp_ctx *c) {
   cudaSetDevice(c->cfg.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void *p : c->allocs) cudaFree(p);
+  if (c->gauss) {
+    gauss_destroy(*c->gauss);
+    delete c->gauss;
+  }
   if (c->staging) cudaFree(c->staging);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_diag) cudaFreeHost(c->h_diag);
@@ -809,8 +959,12 @@ int mp_check_status(mp_ctx *c) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_err(c, e, "status read");
   const int newton = c->h_status[ST_NEWTON], nonfin = c->h_status[ST_NONFINITE];
-  if (newton || nonfin) {
+  const int timeout = c->h_status[ST_TIMEOUT];
+  if (newton || nonfin || timeout) {
     cudaMemsetAsync(c->d_status, 0, ST_COUNT * sizeof(int), c->stream);
+    if (timeout)
+      return set_err(c, MP_ERR_CUDA, "%d blocks gave up waiting for their TMA plane loads; the step is incomplete",
+                     timeout);
     if (nonfin) return set_err(c, MP_ERR_NONFINITE, "%d field values became NaN or Inf", nonfin);
     return set_err(c, MP_ERR_NEWTON, "Kerr Newton solve did not converge in %d cell updates (max %d iterations)",
                    newton, c->cfg.newton_max_iter);

@@ -1,0 +1,299 @@
+// mp_cell.cuh - the arithmetic of one cell's E update and B update, shared by
+// the global-load kernels (mp_step_kernels.cu) and the TMA-staged kernels
+// (mp_step_tma.cu).  The caller loads the field values (from global memory or
+// from shared memory) and the PLRC accumulators, calls e_cell / b_cell, and
+// stores the results; the CPML psi of the faces containing the cell and the
+// injection-plane values are loaded and stored here with plain global accesses
+// (a minority of cells).
+//
+// Order of operations per cell: every load before any store.  The arrays may
+// alias as far as the compiler can tell, so a load written after a store would
+// wait for that store to complete.
+#ifndef MPB_MP_CELL_CUH
+#define MPB_MP_CELL_CUH
+
+#include "mp_device.h"
+
+#include <cuda_runtime.h>
+
+namespace mpb {
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { typedef float2 type; };
+template <> struct Vec2<double> { typedef double2 type; };
+
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+__device__ __forceinline__ bool finite3(double a, double b, double c) {
+  return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
+// (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped.
+__device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
+                                              int *status) {
+  double Eold;
+  int it = 0;
+  do {
+    Eold = E;
+    const double E2 = E * E;
+    E = (2.0 * A * E2 * E + C) / (3.0 * A * E2 + 1.0);
+  } while (fabs(E - Eold) > tol && ++it < maxit);
+  if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
+  return E;
+}
+
+// FDTD_Nonlinear's Newton for eps E + chi E^3 = D (fdtd_nl.cpp:86-92).
+__device__ __forceinline__ double nl_newton(double E, double eps, double chi, double D, double tol,
+                                            int maxit, int *status) {
+  double Eold;
+  int it = 0;
+  do {
+    Eold = E;
+    const double E2 = E * E;
+    E = (2.0 * chi * E2 * E + D) / (3.0 * chi * E2 + eps);
+  } while (fabs(E - Eold) > tol && ++it < maxit);
+  if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
+  return E;
+}
+
+// Values one E update reads: B at the cell and its x-1, y-1, z-1 neighbours
+// (the ones the curl uses) and the old E.
+template <typename T>
+struct EIn {
+  T bx, by, bz;
+  T bz_xm, by_xm, bz_ym, bx_ym, bx_km, by_km;
+  T ex, ey, ez;
+};
+
+// Values one B update reads: E at the cell and its x+1, y+1, z+1 neighbours
+// and the old B.
+template <typename T>
+struct BIn {
+  T ex, ey, ez;
+  T ez_xp, ey_xp, ez_yp, ex_yp, ex_kp, ey_kp;
+  T bx, by, bz;
+};
+
+// One cell of the E half: CPML psi_E (cpml_border.cpp:398-425), the current sum
+// in MPulse's order (fdtd_plrc.t:352-373), the PLRC recursion and the E update
+// of plrcStepD (fdtd_plrc.cpp:94-261, :304-427), FDTD_Plain::stepD
+// (fdtd_plain.cpp:37-77) or FDTD_Nonlinear::stepD (fdtd_nl.cpp:38-100).
+// i, j are 0-based interior indices (MPulse i+1, j+1); k is MPulse's z index.
+// q holds the cell's PLRC accumulators on entry and their new values on exit.
+template <typename T, int MODE, int NP>
+__device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
+                                       const EIn<T> &v, T ikx, T iky, T ikz,
+                                       typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
+                                       T &ezn) {
+  const T dt = p.dt;
+  // ---- loads of the CPML psi of the faces containing the cell, and of the
+  // injection plane
+  T cp0[6], cp1[6], cb[6], cc[6];
+  int cli[6];  // layer arrays hold < 2^31 cells (checked by mp_create)
+  bool cin[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const CpmlFace<T> &F = p.cpml[f];
+    const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
+    cin[f] = (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) && F.active && idx >= F.lo && idx <= F.hi;
+    if (cin[f]) {
+      if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+      else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+      else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
+      cp0[f] = F.psi0[cli[f]];
+      cp1[f] = F.psi1[cli[f]];
+      cb[f] = ld(F.b + idx);
+      cc[f] = ld(F.c + idx);
+    }
+  }
+  T sa = T(0), sb = T(0);
+  bool on_src = false;
+  if (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) {
+    for (int s = 0; s < p.n_src; ++s) {
+      if (k == p.src[s].plane) {
+        sa = ld(p.src[s].v0 + col);
+        sb = ld(p.src[s].v1 + col);
+        on_src = true;
+      }
+    }
+  }
+
+  // ---- E-side currents: CPML faces, then the injector plane
+  T jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (!cin[f]) continue;
+    const int dim = p.cpml[f].dim;
+    T d0, d1;  // differences of B along dim for psi0, psi1
+    if (dim == 2) { d0 = -(v.by - v.by_km); d1 = v.bx - v.bx_km; }
+    else if (dim == 0) { d0 = -(v.bz - v.bz_xm); d1 = v.by - v.by_xm; }
+    else { d0 = -(v.bx - v.bx_ym); d1 = v.bz - v.bz_ym; }
+    cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
+    cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+    if (dim == 2) { jx += cp0[f]; jy += cp1[f]; }
+    else if (dim == 0) { jy += cp0[f]; jz += cp1[f]; }
+    else { jz += cp0[f]; jx += cp1[f]; }
+  }
+  if (on_src) {
+    for (int m = 0; m < p.src_mult; ++m) {
+      jx += sa;
+      jy += sb;
+    }
+  }
+
+  // curl_kappa B (fdtd_plrc.cpp:207-244)
+  const T cbx = (v.bz - v.bz_ym) * iky - (v.by - v.by_km) * ikz;
+  const T cby = (v.bx - v.bx_km) * ikz - (v.bz - v.bz_xm) * ikx;
+  const T cbz = (v.by - v.by_xm) * ikx - (v.bx - v.bx_ym) * iky;
+  const T ex = v.ex, ey = v.ey, ez = v.ez;
+
+  if (MODE == MODE_PLAIN) {
+    exn = ex + dt * cbx;
+    eyn = ey + dt * cby;
+    ezn = ez + dt * cbz;
+  } else if (MODE == MODE_NL) {
+    const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
+    const T f = T(p.eps_d + p.chi_d * E2);
+    const T Dx = f * ex + dt * cbx, Dy = f * ey + dt * cby, Dz = f * ez + dt * cbz;
+    const double D = sqrt((double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz);
+    if (D > 0) {
+      const double E = nl_newton(sqrt(E2), p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status);
+      exn = T(E * Dx / D);
+      eyn = T(E * Dy / D);
+      ezn = T(E * Dz / D);
+    } else {
+      exn = eyn = ezn = T(0);
+    }
+  } else if (!med) {
+    // background: no poles, no Kerr term
+    exn = (p.eps_bg * ex + dt * (cbx + jx)) * p.inv_eps_bg;
+    eyn = (p.eps_bg * ey + dt * (cby + jy)) * p.inv_eps_bg;
+    ezn = (p.eps_bg * ez + dt * (cbz + jz)) * p.inv_eps_bg;
+  } else {
+    T Px = T(0), Py = T(0), Pz = T(0);
+    if (NP > 0) {
+      const T e3[3] = {ex, ey, ez};
+      T P3[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int n = 0; n < NP; ++n) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          // psi~ = (dchi0 - dxi0) e + psi ; Psi += Re psi~
+          const T ar = p.pD[n][0] * e3[c] + q[n][c].x;
+          const T ai = p.pD[n][1] * e3[c] + q[n][c].y;
+          P3[c] += ar;
+          // psi <- dxi0 e + Crec psi~
+          q[n][c].x = p.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
+          q[n][c].y = p.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
+        }
+      }
+      Px = P3[0];
+      Py = P3[1];
+      Pz = P3[2];
+    }
+    if (MODE == MODE_PLRC_LIN) {
+      exn = (p.numer * ex + (dt * (cbx + jx) + Px)) * p.inv_denom;
+      eyn = (p.numer * ey + (dt * (cby + jy) + Py)) * p.inv_denom;
+      ezn = (p.numer * ez + (dt * (cbz + jz) + Pz)) * p.inv_denom;
+    } else {
+      const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
+      const T f = p.numer + p.chi * T(E2);
+      const T cx = (f * ex + dt * (cbx + jx) + Px) * p.inv_denom;
+      const T cy = (f * ey + dt * (cby + jy) + Py) * p.inv_denom;
+      const T cz = (f * ez + dt * (cbz + jz) + Pz) * p.inv_denom;
+      const double C = sqrt((double)cx * cx + (double)cy * cy + (double)cz * cz);
+      if (C > 0) {
+        const double E = kerr_newton(sqrt(E2), p.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
+        exn = T(E * cx / C);
+        eyn = T(E * cy / C);
+        ezn = T(E * cz / C);
+      } else {
+        exn = eyn = ezn = T(0);
+      }
+    }
+  }
+  if (!finite3((double)exn, (double)eyn, (double)ezn)) atomicAdd(p.status + ST_NONFINITE, 1);
+  // ---- CPML stores
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (!cin[f]) continue;
+    p.cpml[f].psi0[cli[f]] = cp0[f];
+    p.cpml[f].psi1[cli[f]] = cp1[f];
+  }
+}
+
+// One cell of the B half: CPML psi_H (cpml_border.cpp:499-527), the magnetic
+// current sum and plrcStepB (fdtd_plrc.cpp:263-293) / FDTD_Plain::stepB.
+// Returns the new B in bxn, byn, bzn.
+template <typename T>
+__device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k, long long col, const BIn<T> &v,
+                                       T ikx, T iky, T iky_bz, T ikz, T &bxn, T &byn, T &bzn) {
+  const T dt = p.dt;
+  T cp0[6], cp1[6], cb[6], cc[6];
+  int cli[6];
+  bool cin[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const CpmlFace<T> &F = p.cpml[f];
+    const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
+    cin[f] = F.active && idx >= F.lo && idx <= F.hi;
+    if (cin[f]) {
+      if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+      else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+      else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
+      cp0[f] = F.psi0[cli[f]];
+      cp1[f] = F.psi1[cli[f]];
+      cb[f] = ld(F.b + idx);
+      cc[f] = ld(F.c + idx);
+    }
+  }
+  T sa = T(0), sb = T(0);
+  bool on_src = false;
+  for (int s = 0; s < p.n_src; ++s) {
+    if (k == p.src[s].plane) {
+      sa = ld(p.src[s].v0 + col);
+      sb = ld(p.src[s].v1 + col);
+      on_src = true;
+    }
+  }
+
+  // ---- H-side currents (cpml_border.cpp:499-527, incsource.t:112-145)
+  T mx = T(0), my = T(0), mz = T(0);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (!cin[f]) continue;
+    const int dim = p.cpml[f].dim;
+    T d0, d1;
+    if (dim == 2) { d0 = v.ey_kp - v.ey; d1 = -(v.ex_kp - v.ex); }
+    else if (dim == 0) { d0 = v.ez_xp - v.ez; d1 = -(v.ey_xp - v.ey); }
+    else { d0 = v.ex_yp - v.ex; d1 = -(v.ez_yp - v.ez); }
+    cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
+    cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+    if (dim == 2) { mx += cp0[f]; my += cp1[f]; }
+    else if (dim == 0) { my += cp0[f]; mz += cp1[f]; }
+    else { mz += cp0[f]; mx += cp1[f]; }
+  }
+  if (on_src) {
+    for (int m = 0; m < p.src_mult; ++m) {
+      mx += sa;
+      my += sb;
+    }
+  }
+
+  // ---- plrcStepB (fdtd_plrc.cpp:263-293)
+  bxn = v.bx + dt * ((v.ey_kp - v.ey) * ikz - (v.ez_yp - v.ez) * iky + mx);
+  byn = v.by + dt * ((v.ez_xp - v.ez) * ikx - (v.ex_kp - v.ex) * ikz + my);
+  bzn = v.bz + dt * ((v.ex_yp - v.ex) * iky_bz - (v.ey_xp - v.ey) * ikx + mz);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (!cin[f]) continue;
+    p.cpml[f].psi0[cli[f]] = cp0[f];
+    p.cpml[f].psi1[cli[f]] = cp1[f];
+  }
+}
+
+}  // namespace mpb
+
+#endif

@@ -12,6 +12,8 @@
 #ifndef MPB_MP_DEVICE_H
 #define MPB_MP_DEVICE_H
 
+#include <cuda.h>  // CUtensorMap (a type only; no driver call is linked)
+
 #include <cstddef>
 #include <cstdint>
 
@@ -22,7 +24,19 @@ enum Mode { MODE_PLAIN = 0, MODE_NL = 1, MODE_PLRC_LIN = 2, MODE_PLRC_NONLIN = 3
 enum Face { FACE_NORTH = 0, FACE_SOUTH, FACE_WEST, FACE_EAST, FACE_UP, FACE_DOWN };
 
 // Device status word, read back after mp_step.
-enum StatusSlot { ST_NEWTON = 0, ST_NONFINITE = 1, ST_COUNT = 4 };
+enum StatusSlot { ST_NEWTON = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_COUNT = 4 };
+
+// Tile of the TMA-staged kernels (mp_step_tma.cu): 32 x 8 columns.
+static const int kTmaTileX = 32, kTmaTileY = 8;
+
+// Tensor maps of the TMA-staged kernels, one per array and halo shape.
+struct ETmaMaps {
+  CUtensorMap bx, by, bz, ex, ey, ez;
+  CUtensorMap psi[3][3];
+};
+struct BTmaMaps {
+  CUtensorMap ex, ey, ez, bx, by, bz;
+};
 
 // One CPML current (CPMLBorderECurrent / CPMLBorderHCurrent,
 // cpml_border.cpp:345-527) restricted to the cells the kernels update.  Its two
@@ -100,6 +114,7 @@ struct BParams {
   int n_src;
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
+  int *status;
 };
 
 // Incident-source plane evaluation.
@@ -117,6 +132,13 @@ struct SourceEvalParams {
   double centre[3];
   const double *w_coef;   // Faddeeva expansion coefficients (highest power first)
   double w_L;
+  // gauss_inject: the planes [Nt][ny][nx] of the block that starts at g_toff
+  // (getHField: Bx in g_f1; getEField: Ex in g_f1, Ey in g_f2), scaled by
+  // g_scale; zero fields while g_active is 0
+  const double *g_f1, *g_f2;
+  double g_scale;
+  long long g_toff;
+  int g_active;
 };
 
 }  // namespace mpb

@@ -69,14 +69,30 @@ __device__ void short_pulse_field(const SourceEvalParams &q, int i, int j, int l
   }
 }
 
+// GaussInjectSourceFunc::getHField / getEField (gaussinject.cpp:204-222) on
+// the block precomputed by mp_gauss_kernels.cu.
+__device__ void gauss_beam_field(const SourceEvalParams &q, int i, int j, double out[3]) {
+  out[0] = out[1] = out[2] = 0.0;
+  if (!q.g_active) return;
+  const long long o = (q.time - q.g_toff) * ((long long)q.nx * q.ny) + (long long)j * q.nx + i;
+  out[0] = q.g_scale * q.g_f1[o];
+  if (q.isH) out[1] = q.g_scale * q.g_f2[o];
+}
+
+// The incident field at interior column (i, j) (0-based; MPulse i + 1, j + 1).
+__device__ void source_field(const SourceEvalParams &q, int i, int j, double f[3]) {
+  if (q.kind == 3) short_pulse_field(q, i + 1, j + 1, q.l, f);
+  else if (q.kind == 5) gauss_beam_field(q, i, j, f);
+  else plane_source_field(q, i + 1, j + 1, q.l, f);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) source_plane_kernel(const SourceEvalParams q, T *v0, T *v1) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= q.nx || j >= q.ny) return;
   double f[3];
-  if (q.kind == 3) short_pulse_field(q, i + 1, j + 1, q.l, f);
-  else plane_source_field(q, i + 1, j + 1, q.l, f);
+  source_field(q, i, j, f);
   const long long col = (long long)j * q.nx + i;
   // J0 = F[t2] / DX, J1 = F[t1] / DX with (t1, t2) = (x, y) on z faces
   v0[col] = T(f[1] / q.DX);
@@ -90,7 +106,40 @@ cudaError_t launch_source_plane(const SourceEvalParams &q, T *v0, T *v1, cudaStr
   return cudaGetLastError();
 }
 
+// The planes of `nsteps` consecutive steps in one launch: the values depend
+// only on Process::time, so step t0 + q's E-side pair goes to
+// out + (4 q + 0, 1) * plane and its H-side pair to out + (4 q + 2, 3) * plane.
+template <typename T>
+__global__ void __launch_bounds__(256) source_batch_kernel(const SourceEvalParams qe, const SourceEvalParams qh,
+                                                          long long t0, T *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= qe.nx || j >= qe.ny) return;
+  const int step = blockIdx.z >> 1, side = blockIdx.z & 1;
+  SourceEvalParams q = side ? qh : qe;
+  q.time = t0 + step;
+  double f[3];
+  source_field(q, i, j, f);
+  const long long plane = (long long)qe.nx * qe.ny;
+  const long long col = (long long)j * qe.nx + i;
+  T *v0 = out + (4LL * step + 2 * side) * plane;
+  v0[col] = T(f[1] / q.DX);
+  v0[plane + col] = T(f[0] / q.DX);
+}
+
+template <typename T>
+cudaError_t launch_source_batch(const SourceEvalParams &qe, const SourceEvalParams &qh, long long t0, int nsteps,
+                                T *out, cudaStream_t st) {
+  const dim3 b(32, 8, 1), g((qe.nx + 31) / 32, (qe.ny + 7) / 8, 2 * nsteps);
+  source_batch_kernel<T><<<g, b, 0, st>>>(qe, qh, t0, out);
+  return cudaGetLastError();
+}
+
 template cudaError_t launch_source_plane<float>(const SourceEvalParams &, float *, float *, cudaStream_t);
 template cudaError_t launch_source_plane<double>(const SourceEvalParams &, double *, double *, cudaStream_t);
+template cudaError_t launch_source_batch<float>(const SourceEvalParams &, const SourceEvalParams &, long long, int,
+                                                float *, cudaStream_t);
+template cudaError_t launch_source_batch<double>(const SourceEvalParams &, const SourceEvalParams &, long long, int,
+                                                 double *, cudaStream_t);
 
 }  // namespace mpb

@@ -65,6 +65,17 @@ ParameterMap *GpuSourceBlock::MakeParamMap(ParameterMap *pm) {
     (*pm)["amp"] = WParameter(new ParameterValue<double>(&amp, 1));
     (*pm)["eps"] = WParameter(new ParameterValue<double>(&eps, 1));
   }
+  if (kind == MP_SOURCE_GAUSS_BEAM) {  // GaussInject::MakeParamMap (gaussinject.cpp:33-49)
+    (*pm)["SizeT"] = WParameter(new ParameterValue<int>(&SizeT, 4096));
+    (*pm)["length"] = WParameter(new ParameterValue<double>(&length, 1.));
+    (*pm)["width"] = WParameter(new ParameterValue<double>(&width, 1.));
+    (*pm)["k0"] = WParameter(new ParameterValue<double>(&k0, 2 * M_PI));
+    (*pm)["Shift"] = WParameter(new ParameterValue<double>(&Shift, 0));
+    (*pm)["Time"] = WParameter(new ParameterValue<double>(&Time, 0));
+    (*pm)["amp"] = WParameter(new ParameterValue<double>(&amp, 1));
+    (*pm)["eps"] = WParameter(new ParameterValue<double>(&eps, 1));
+    (*pm)["toff"] = WParameter(new ParameterValue<int>(&toff, 0));
+  }
   return pm;
 }
 
@@ -88,6 +99,10 @@ void GpuSourceBlock::fill(mp_source &s) const {
   if (kind == MP_SOURCE_SHORT_PULSE) {
     s.length = length; s.waist = waist; s.om0 = om0;
     s.t_shift = TShift; s.z_shift = ZShift; s.phase = Phase; s.amp = amp; s.eps = eps;
+  }
+  if (kind == MP_SOURCE_GAUSS_BEAM) {
+    s.t_size = SizeT; s.length = length; s.width = width; s.k0 = k0; s.shift = Shift;
+    s.time = Time; s.amp = amp; s.eps = eps; s.t_off = toff;
   }
 }
 
@@ -129,6 +144,8 @@ ParameterMap *FDTD_GPU::MakeParamMap(ParameterMap *pm) {
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_PLANE_GAUSS>, CurrentFactory>(&blocks));
   (*pm)["short_pulse_inject"] =
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_SHORT_PULSE>, CurrentFactory>(&blocks));
+  (*pm)["gauss_inject"] =
+      WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_GAUSS_BEAM>, CurrentFactory>(&blocks));
   return pm;
 }
 

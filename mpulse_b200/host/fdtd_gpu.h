@@ -63,6 +63,8 @@ class GpuSourceBlock : public CurrentFactory {
   double kx, ky, kz, Hx, Hy, Hz, Hx_bg, Hy_bg, Hz_bg, Ex_bg, Ey_bg, Ez_bg;
   double ramp, width, offset, eps;
   double length, waist, om0, TShift, ZShift, Phase, amp;
+  int SizeT, toff;
+  double k0, Shift, Time;
   void fill(mp_source &s) const;
 
  protected:

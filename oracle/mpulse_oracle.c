@@ -61,12 +61,27 @@ typedef struct {
   int off[3];
 } inc_layer;
 
+/* One GaussInjectSourceFunc (gaussinject.cpp:56-482): an angular-spectrum
+ * Gaussian beam whose injection-plane fields are precomputed for blocks of Nt
+ * steps by transforms over t, y and x.  isH = 0 holds Bx (for the E current's
+ * getHField), isH = 1 holds Ex in F1 and Ey in F2 (for the H current). */
+typedef struct {
+  int isH;
+  int SizeT, SizeX, SizeY, SizeTH, SizeXH, SizeYH, Nt, toff, blockCount, blockToff, active;
+  long long computed; /* block held in F1/F2, -1 for none */
+  double length, width, k0, Shift, Time, Time0, amp, eps, lightspeed, DX, DY, DT, BoxX, BoxY, BoxT;
+  double sx, sy, sz;
+  double *F1, *F2; /* [SizeX][SizeY][Nt] */
+} gauss_state;
+
 typedef struct {
   /* precomputed per source (sources.cpp:14-56, shortpulseinject.cpp:56-113) */
   double E[3];       /* plane sources: E amplitude vector */
   double om;
   /* short pulse */
   double lightspeed, ZRl, amp, phase, tshift, zshift, centre[3];
+  /* gauss_inject: [0] the E current's state, [1] the H current's */
+  gauss_state gs[2];
 } src_state;
 
 typedef struct mpo_sim {
@@ -271,6 +286,180 @@ static double complex sp_bfunc(const src_state *st, const mp_source *s, double x
 }
 
 /* ------------------------------------------------------------------------ */
+/* gauss_inject: GaussInjectSourceFunc (gaussinject.cpp:56-482) and its
+ * GaussFunc helpers (gaussinject.h:166-203). */
+
+static double gf_gauss(const gauss_state *g, double x, double y, double z) {
+  const double zoff = z - g->k0;
+  return exp(-0.25 * zoff * zoff * g->length * g->length - 0.25 * (x * x + y * y) * g->width * g->width);
+}
+static double gf_shift(const gauss_state *g, double x, double y, double z) {
+  return -(x * g->sx + y * g->sy + z * g->sz);
+}
+static double gf_kp(double x, double z) { return sqrt(x * x + z * z); }
+static double gf_k(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+static double gf_comp(int which, double x, double y, double z) {
+  if (which == 0) { /* excomp */
+    const double D = gf_k(x, y, z) * gf_kp(x, z);
+    return D == 0 ? 0 : (-x * y / D);
+  }
+  if (which == 1) { /* eycomp */
+    const double D = gf_k(x, y, z);
+    return D == 0 ? 0 : (gf_kp(x, z) / D);
+  }
+  const double D = gf_kp(x, z); /* bxcomp */
+  return D == 0 ? 0 : (-z / D);
+}
+static int gf_sign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+/* Unnormalised DFT with FFTW's conventions: out[k] = sum_j in[j] e^{sign 2 pi i jk/n}. */
+static void dft(const double complex *in, double complex *out, int n, int sign) {
+  for (int k = 0; k < n; ++k) {
+    double complex s = 0;
+    for (int j = 0; j < n; ++j) {
+      const double a = sign * 2.0 * M_PI * (double)(((long long)j * k) % n) / n;
+      s += in[j] * CMPLX(cos(a), sin(a));
+    }
+    out[k] = s;
+  }
+}
+
+/* fillEx / fillEy / fillBx (gaussinject.cpp:329-482) with transformT / Y / X
+ * (:257-327): the angular spectrum at (kx, ky, omega), backward transform over
+ * omega (only the Nt samples of the current block kept), forward transforms
+ * over ky and kx, real part. */
+static void gauss_fill(gauss_state *g, int which, double *F) {
+  const int SX = g->SizeX, SY = g->SizeY, ST = g->SizeT, Nt = g->Nt;
+  double complex *A = malloc(sizeof(double complex) * ST);
+  double complex *uo = malloc(sizeof(double complex) * ST), *ut = malloc(sizeof(double complex) * ST);
+  double complex *uy_in = malloc(sizeof(double complex) * SY), *uy = malloc(sizeof(double complex) * SY);
+  double complex *ux_in = malloc(sizeof(double complex) * SX), *ux = malloc(sizeof(double complex) * SX);
+  double complex *tmpTY = malloc(sizeof(double complex) * SY * Nt);
+  double complex *tmpTX = malloc(sizeof(double complex) * SX * SY * Nt);
+  const int blockmin = g->blockCount * Nt;
+  for (int i = 0; i < SX; ++i) {
+    for (int j = 0; j < SY; ++j) {
+      for (int k = 0; k < ST; ++k) {
+        const double kx = 2 * M_PI * (i - g->SizeXH) / (g->BoxX);
+        const double ky = 2 * M_PI * (j - g->SizeYH) / (g->BoxY);
+        const double om = 2 * M_PI * (k - g->SizeTH) / (g->BoxT);
+        double K = om * om - ky * ky - kx * kx;
+        if (fabs(K) < 1e-9) K = 0;
+        if (K < 0) A[k] = 0;
+        else {
+          const double kz = sqrt(K) * gf_sign(om);
+          const double a = gf_comp(which, kx, ky, kz) * gf_gauss(g, kx, ky, kz);
+          const double ph = gf_shift(g, kx, ky, kz) + 0.5 * M_PI;
+          A[k] = a * cexp(-I * (ph + g->Time * om));
+        }
+      }
+      /* transformT */
+      const double fT = (2 * M_PI * g->length / g->BoxT);
+      for (int k = 0; k < ST; ++k) uo[k] = A[(k + g->SizeTH) % ST];
+      dft(uo, ut, ST, +1);
+      for (int kh = 0; kh < Nt; ++kh) tmpTY[j * Nt + kh] = fT * ut[(kh + blockmin + g->SizeTH) % ST];
+    }
+    /* transformY */
+    const double fY = (g->width / g->BoxY);
+    for (int k = 0; k < Nt; ++k) {
+      for (int j = 0; j < SY; ++j) uy_in[(j + g->SizeYH) % SY] = tmpTY[j * Nt + k];
+      dft(uy_in, uy, SY, -1);
+      for (int j = 0; j < SY; ++j) tmpTX[((size_t)i * SY + j) * Nt + k] = fY * uy[(j + g->SizeYH) % SY];
+    }
+  }
+  /* transformX */
+  const double fX = (g->width / g->BoxX);
+  for (int j = 0; j < SY; ++j)
+    for (int k = 0; k < Nt; ++k) {
+      for (int i = 0; i < SX; ++i) ux_in[(i + g->SizeXH) % SX] = tmpTX[((size_t)i * SY + j) * Nt + k];
+      dft(ux_in, ux, SX, -1);
+      for (int i = 0; i < SX; ++i) F[((size_t)i * SY + j) * Nt + k] = fX * creal(ux[(i + g->SizeXH) % SX]);
+    }
+  free(A); free(uo); free(ut); free(uy_in); free(uy); free(ux_in); free(ux); free(tmpTY); free(tmpTX);
+}
+
+/* GaussInjectSourceFunc::setTime (gaussinject.cpp:152-184).  The reference
+ * computes block c = 0, 1, .. when the time reaches toff + c Nt and switches
+ * off at the first block start at or past toff + SizeT, so for times that step
+ * by one the state at time t is: inactive before toff, block
+ * b = (t - toff) / Nt while b Nt < SizeT, inactive after.  That function of t
+ * is what is computed here; it also covers times set directly, where the
+ * reference's block counter would index outside its block. */
+static void gauss_set_time(gauss_state *g, long long time) {
+  if (time < g->toff) {
+    g->active = 0;
+    return;
+  }
+  const long long b = (time - g->toff) / g->Nt;
+  if (b * g->Nt >= g->SizeT) {
+    g->active = 0;
+    return;
+  }
+  g->active = 1;
+  if (g->computed == b) return;
+  g->blockCount = (int)b;
+  if (!g->isH) {
+    g->sx = 0; g->sy = 0.5 * g->DX; g->sz = g->Shift + 0.5 * g->DX;
+    gauss_fill(g, 2, g->F1);
+  } else {
+    /* Time -= DT/2 for the fills and += DT/2 after them, once per block: block
+     * b sees Time moved by b such round trips */
+    double T = g->Time0;
+    for (long long n = 0; n < b; ++n) T = (T - 0.5 * g->DT) + 0.5 * g->DT;
+    g->Time = T - 0.5 * g->DT;
+    g->sx = 0.5 * g->DX; g->sy = 0; g->sz = g->Shift;
+    gauss_fill(g, 0, g->F1);
+    g->sx = 0; g->sy = 0.5 * g->DX; g->sz = g->Shift;
+    gauss_fill(g, 1, g->F2);
+  }
+  g->blockToff = g->toff + g->blockCount * g->Nt;
+  g->computed = b;
+}
+
+/* GaussInjectSourceFunc::setParam / initSourceFunc (gaussinject.cpp:56-150). */
+static void gauss_init(gauss_state *g, const mp_source *p, const mp_config *c, int isH) {
+  memset(g, 0, sizeof(*g));
+  g->isH = isH;
+  g->SizeT = p->t_size;
+  g->length = p->length;
+  g->width = p->width;
+  g->k0 = p->k0;
+  g->Shift = p->shift;
+  g->Time = p->time;
+  g->Time0 = p->time;
+  g->amp = p->amp;
+  g->eps = p->eps;
+  g->toff = p->t_off;
+  g->lightspeed = sqrt(1 / g->eps);
+  g->SizeX = c->nx + 2;
+  g->SizeY = c->ny + 2;
+  g->SizeTH = g->SizeT / 2;
+  g->SizeXH = g->SizeX / 2;
+  g->SizeYH = g->SizeY / 2;
+  g->DX = c->dx;
+  g->DY = c->dy;
+  g->DT = c->dt * g->lightspeed;
+  g->BoxX = g->SizeX * g->DX;
+  g->BoxY = g->SizeY * g->DY;
+  g->BoxT = g->SizeT * g->DT;
+  g->blockCount = 0;
+  g->blockToff = g->toff;
+  g->active = 0;
+  g->computed = -1;
+  /* initSourceFunc (gaussinject.cpp:142): high[2] - low[2] of the storage,
+   * whose z range is 0..nz+1 */
+  g->Nt = 1 << (int)round(log((double)(c->nz + 1)) / log(2.0) + 1e-6);
+  const size_t n = (size_t)g->SizeX * g->SizeY * g->Nt;
+  g->F1 = calloc(n, sizeof(double));
+  g->F2 = calloc(n, sizeof(double));
+}
+
+static double gauss_value(const gauss_state *g, const double *F, int i, int j, long long time) {
+  const long long t = time - g->blockToff;
+  return F[((size_t)i * g->SizeY + j) * g->Nt + (size_t)t];
+}
+
+/* ------------------------------------------------------------------------ */
 /* Source functions: the field a TF/SF current needs at cell (i, j, l). */
 
 /* PlaneWaveSourceEFunc::getHField (sources.cpp:107-125) and
@@ -312,6 +501,14 @@ static void src_hfield(const mpo_sim *s, int n, int i, int j, int l, long long t
     h[2] = 0.0;
     return;
   }
+  if (p->kind == MP_SOURCE_GAUSS_BEAM) {
+    /* GaussInjectSourceFunc::getHField (gaussinject.cpp:215-223) */
+    const gauss_state *g = &st->gs[0];
+    h[0] = g->active ? sqrt(g->eps) * g->amp * gauss_value(g, g->F1, i, j, time) : 0.0;
+    h[1] = 0.0;
+    h[2] = 0.0;
+    return;
+  }
   h[0] = h[1] = h[2] = 0.0;
 }
 
@@ -349,6 +546,14 @@ static void src_efield(const mpo_sim *s, int n, int i, int j, int l, long long t
     const double posTime = (double)time * dt - st->tshift;
     e[0] = st->amp * creal(sp_efunc(st, p, posxh, posyo, poszo, posTime));
     e[1] = 0.0;
+    e[2] = 0.0;
+    return;
+  }
+  if (p->kind == MP_SOURCE_GAUSS_BEAM) {
+    /* GaussInjectSourceFunc::getEField (gaussinject.cpp:205-213) */
+    const gauss_state *g = &st->gs[1];
+    e[0] = g->active ? g->amp * gauss_value(g, g->F1, i, j, time) : 0.0;
+    e[1] = g->active ? g->amp * gauss_value(g, g->F2, i, j, time) : 0.0;
     e[2] = 0.0;
     return;
   }
@@ -661,6 +866,8 @@ static void add_layer(mpo_sim *s, double **tot, const box3 *b, int comp[2], doub
  * whose values the shared grid holds. */
 static void inc_add(mpo_sim *s, inc_layer *L, int writer, double **tot) {
   const box3 *b = &L->box;
+  /* SourceFunc::setTime at the start of stepScheme (incsource.t:52-53, :124-125) */
+  if (s->cfg.sources[writer].kind == MP_SOURCE_GAUSS_BEAM) gauss_set_time(&s->src[writer].gs[L->isH], s->time);
   for (int k = b->lo[2]; k <= b->hi[2]; ++k)
     for (int j = b->lo[1]; j <= b->hi[1]; ++j)
       for (int i = b->lo[0]; i <= b->hi[0]; ++i) {
@@ -976,6 +1183,14 @@ int mpo_create(const mp_config *cfg, mpo_sim **out) {
       st->phase = 2 * M_PI * p->phase;
       st->tshift = p->t_shift;
       st->zshift = p->z_shift;
+    } else if (p->kind == MP_SOURCE_GAUSS_BEAM) {
+      if (p->t_size < 2 || p->eps <= 0) {
+        snprintf(g_create_err, sizeof g_create_err, "gauss beam needs t_size >= 2 and eps > 0");
+        mpo_destroy(s);
+        return MP_ERR_INVALID;
+      }
+      gauss_init(&st->gs[0], p, cfg, 0);
+      gauss_init(&st->gs[1], p, cfg, 1);
     } else {
       snprintf(g_create_err, sizeof g_create_err, "source kind %d is not available in the oracle", p->kind);
       mpo_destroy(s);
@@ -1000,6 +1215,8 @@ void mpo_destroy(mpo_sim *s) {
   for (int c = 0; c < 3; ++c) { free(s->Jt[c]); free(s->Mt[c]); free(s->kapE[c]); free(s->kapH[c]); }
   for (int l = 0; l < s->nE; ++l) { free(s->Elay[l].psi[0]); free(s->Elay[l].psi[1]); free(s->Elay[l].b); free(s->Elay[l].c); }
   for (int l = 0; l < s->nH; ++l) { free(s->Hlay[l].psi[0]); free(s->Hlay[l].psi[1]); free(s->Hlay[l].b); free(s->Hlay[l].c); }
+  for (int q = 0; q < MP_MAX_SOURCES; ++q)
+    for (int h = 0; h < 2; ++h) { free(s->src[q].gs[h].F1); free(s->src[q].gs[h].F2); }
   free(s);
 }
 
@@ -1102,6 +1319,7 @@ void mpo_faddeeva(const double *re, const double *im, double *wre, double *wim, 
  * which = 0 -> getHField (E current), 1 -> getEField (H current). */
 int mpo_source_field(mpo_sim *s, int src, int which, int i, int j, int l, long long time, double out[3]) {
   if (src < 0 || src >= s->cfg.n_sources) return MP_ERR_INVALID;
+  if (s->cfg.sources[src].kind == MP_SOURCE_GAUSS_BEAM) gauss_set_time(&s->src[src].gs[which ? 1 : 0], time);
   if (which) src_efield(s, src, i, j, l, time, out);
   else src_hfield(s, src, i, j, l, time, out);
   return MP_OK;

@@ -179,6 +179,12 @@ def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver
                     f"d {s.distance}", f"length {_fmt(s.length)}", f"width {_fmt(s.waist)}",
                     f"om0 {_fmt(s.om0)}", f"TShift {_fmt(s.t_shift)}", f"ZShift {_fmt(s.z_shift)}",
                     f"Phase {_fmt(s.phase)}", f"amp {_fmt(s.amp)}", f"eps {_fmt(s.eps)}"]) + " }")
+            elif s.kind == abi.MP_SOURCE_GAUSS_BEAM:
+                body.append("gauss_inject { " + " ".join([
+                    f"d {s.distance}", f"SizeT {s.t_size}", f"length {_fmt(s.length)}",
+                    f"width {_fmt(s.width)}", f"k0 {_fmt(s.k0)}", f"Shift {_fmt(s.shift)}",
+                    f"Time {_fmt(s.time)}", f"amp {_fmt(s.amp)}", f"eps {_fmt(s.eps)}",
+                    f"toff {s.t_off}"]) + " }")
             else:
                 raise ValueError(f"source kind {s.kind} has no runnable reference plug-in")
     if extra:

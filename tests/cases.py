@@ -54,6 +54,8 @@ def make_case(name: str, precision: int = abi.MP_FP64) -> abi.Config:
         s.z_shift = -0.1
         s.phase = 0.1
         s.amp = 1.0
+        for key, val in spec.get("src", {}).items():
+            setattr(s, key, val)
     return c
 
 
@@ -79,6 +81,28 @@ CASES = {
     "lin_thick_cpml_overlap": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(9, 10, 11), cpml=P.MP_CPML_ALL, cpml_d=7),
     "nonlin_one_pole_periodic": dict(solver=P.MP_SOLVER_PLRC_NONLIN, boundary=P.MP_BOUNDARY_PERIODIC,
                                      poles=(configs.lorentz_pole(0.5, 0.1),), chi=0.4),
+    # gauss_inject: Nt = 16 steps per spectral block for nz = 14.  The first
+    # starts at t_off = 2 and is the only block (t_size 16): zero before, zero
+    # after.  The second crosses two block boundaries and wraps in t.
+    "lin_cpmlz_gauss_beam": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(12, 10, 14), cpml=P.MP_CPML_Z, cpml_d=3,
+                                 medium=(8, 40), sources=(P.MP_SOURCE_GAUSS_BEAM,), src_d=5,
+                                 src=dict(t_size=16, t_off=2, length=0.15, width=0.08, k0=2 * math.pi / 0.8,
+                                          time=0.1, shift=0.02, amp=0.7)),
+    "nonlin_all_gauss_beam_blocks": dict(solver=P.MP_SOLVER_PLRC_NONLIN, n=(16, 8, 14), cpml=P.MP_CPML_ALL,
+                                         cpml_d=3, chi=0.2, medium=(9, 40), sources=(P.MP_SOURCE_GAUSS_BEAM,),
+                                         src_d=6, src=dict(t_size=40, t_off=0, length=0.2, width=0.1,
+                                                           k0=2 * math.pi / 0.7, time=0.2, shift=-0.03,
+                                                           amp=1.1, eps=1.2)),
+    # x a multiple of 32 and y of 8: these run the TMA-staged kernels
+    "tma_nonlin_all_short": dict(solver=P.MP_SOLVER_PLRC_NONLIN, n=(32, 16, 20), cpml=P.MP_CPML_ALL, cpml_d=4,
+                                 chi=0.2, medium=(6, 30), sources=(P.MP_SOURCE_SHORT_PULSE,), src_d=5),
+    "tma_lin_periodic_three_poles": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(64, 8, 18),
+                                         boundary=P.MP_BOUNDARY_PERIODIC, eps=1.3, cpml=P.MP_CPML_Z, cpml_d=3,
+                                         poles=configs.SILICA_POLES + (configs.lorentz_pole(0.3, 0.3, 0.01),),
+                                         sources=(P.MP_SOURCE_PLANE_WAVE,), src_d=5),
+    "tma_plain_xy": dict(solver=P.MP_SOLVER_PLAIN, n=(32, 24, 12)),
+    "tma_nl_xy": dict(solver=P.MP_SOLVER_NL, n=(64, 16, 10), chi=0.3, eps=1.5),
+    "tma_lin_vacuum_cpmlz": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(32, 8, 16), poles=(), cpml=P.MP_CPML_Z),
 }
 
 

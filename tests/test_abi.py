@@ -70,3 +70,11 @@ def test_null_arguments():
     assert L.mp_create(None, None) == abi.MP_ERR_INVALID
     assert L.mp_step(None, 1) == abi.MP_ERR_INVALID
     assert L.mp_launch_count(None) == -1
+
+
+def test_tma_staging_needs_tile_multiples():
+    cfg = abi.default_config()
+    cfg.nx, cfg.ny, cfg.nz = 20, 16, 8
+    cfg.staging = abi.MP_STAGING_TMA
+    rc, msg = _create_error(cfg)
+    assert rc == abi.MP_ERR_UNSUPPORTED and "multiple of 32" in msg

@@ -24,7 +24,7 @@ GPU_NAMES = {
 
 
 @pytest.mark.parametrize("case", ["nonlin_all_short", "lin_split_cpmlz_gauss", "plain_xy", "nl_periodic",
-                                  "nonlin_three_poles"])
+                                  "nonlin_three_poles", "nonlin_all_gauss_beam_blocks"])
 def test_mpulse_driver_with_gpu_solver(case):
     cfg = make_case(case, abi.MP_FP64)
     init = random_fields(cfg, seed=21)

@@ -113,6 +113,29 @@ def test_time_counter_and_sources_follow_process_time():
             assert rel_l2(g.download(n), o.download(n)) <= TOL_FP64
 
 
+@pytest.mark.parametrize("start,steps", [(21, 30), (0, 60), (45, 8)])
+def test_gauss_beam_blocks_follow_process_time(start, steps):
+    """gauss_inject with Nt = 16 and t_size = 40: blocks start at 0, 16, 32 and
+    the source is off from 48 on.  Entering mid-block through mp_set_time
+    computes the block holding the time; stepping on crosses into the next block
+    and past the switch-off like the oracle."""
+    cfg = make_case("nonlin_all_gauss_beam_blocks", abi.MP_FP64)
+    init = random_fields(cfg, seed=11 + start, scale=0.05)
+    o = pyoracle.OracleSim(cfg)
+    for n, v in init.items():
+        o.upload(n, v)
+    o.time = start
+    assert o.step(steps) == abi.MP_OK
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.time = start
+        g.step(steps)
+        for n in abi.FIELD_NAMES:
+            err = rel_l2(g.download(n), o.download(n))
+            assert err <= TOL_FP64, f"{n}: rel-L2 {err:.3e}"
+
+
 @pytest.mark.parametrize("precision,tol", [(abi.MP_FP64, 1e-13), (abi.MP_FP32, 1e-5)])
 def test_field_energy_matches_oracle(precision, tol):
     """mp_field_energy against the oracle's restatement of
@@ -131,3 +154,32 @@ def test_field_energy_matches_oracle(precision, tol):
         e = g.field_energy()
     ref = o.field_energy()
     assert abs(e - ref) <= tol * abs(ref)
+
+
+@pytest.mark.parametrize("precision", [abi.MP_FP64, abi.MP_FP32])
+@pytest.mark.parametrize("case", sorted(c for c in CASES if c.startswith("tma_")))
+def test_tma_and_global_kernels_agree_bitwise(case, precision):
+    """The TMA-staged kernels and the global-load kernels run the same cell
+    arithmetic on the same values: results are identical bit for bit."""
+    out = []
+    for staging in (abi.MP_STAGING_TMA, abi.MP_STAGING_GLOBAL):
+        cfg = make_case(case, precision)
+        cfg.staging = staging
+        init = random_fields(cfg, seed=51)
+        with runtime.Simulation(cfg) as g:
+            for n, v in init.items():
+                g.upload(n, v)
+            g.step(9)
+            out.append({n: g.download(n) for n in abi.FIELD_NAMES})
+    for n in abi.FIELD_NAMES:
+        np.testing.assert_array_equal(out[0][n], out[1][n], err_msg=n)
+
+
+@pytest.mark.parametrize("case", ["tma_nonlin_all_short", "tma_lin_periodic_three_poles"])
+def test_tma_kernels_match_oracle(case):
+    cfg = make_case(case, abi.MP_FP64)
+    cfg.staging = abi.MP_STAGING_TMA
+    init = random_fields(cfg, seed=52)
+    got, want = run_pair(cfg, init, STEPS)
+    for n in abi.FIELD_NAMES:
+        assert rel_l2(got[n], want[n]) <= TOL_FP64, n

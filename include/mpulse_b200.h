@@ -188,7 +188,42 @@ typedef struct mp_config {
 
   int staging;              /* mp_staging: kernel form (results are the same) */
   int device;               /* CUDA device ordinal */
+
+  /* Design region, an addition to MPulse (whose medium parameters are global
+   * scalars, src/fdtd_plrc.h:82-90): in the box of MPulse cells
+   * design_box = {x0, x1, y0, y1, z0, z1} (inclusive; empty when x0 > x1)
+   * every cell has its own eps_infinity, a factor on the Delta epsilon of
+   * every pole and a factor on chi.  They are uploaded by name as "DesignEps",
+   * "DesignDepsScale" and "DesignChiScale", box-sized arrays with x fastest
+   * (defaults: eps, 1, 1).  PLRC solvers only; the box lies inside the medium
+   * planes and the interior.  A cell with factors 1 and eps_infinity = eps
+   * gives the same results as a cell outside the box. */
+  int design_box[6];
 } mp_config;
+
+/* Objectives of mp_objective / mp_adjoint (additions to MPulse). */
+typedef enum mp_objective_kind {
+  /* J = dt * sum over the steps n = 1..T of the sum over the cells of box of
+   * Ex^2 + Ey^2 + Ez^2 after step n */
+  MP_OBJ_E2_BOX = 1,
+  /* J = dt * dx * dy * sum over n = 1..T of the sum over the x-y range of box
+   * at the plane z = box[4] of Ex By - Ey Bx after step n (cell-centred
+   * product of the stored components, no Yee interpolation) */
+  MP_OBJ_SZ_PLANE = 2
+} mp_objective_kind;
+
+typedef struct mp_adjoint_config {
+  int kind;               /* mp_objective_kind */
+  int box[6];             /* x0, x1, y0, y1, z0, z1, MPulse cells, inclusive */
+  int steps;              /* T: steps of the forward run */
+  /* The forward state is saved every checkpoint_every steps; the reverse pass
+   * recomputes each segment from its checkpoint, keeping E of every step of
+   * the segment.  0 chooses the segment length from mem_budget (bytes of
+   * device memory for checkpoints and the segment's E history; 0 = no limit,
+   * which keeps all steps in one segment). */
+  int checkpoint_every;
+  double mem_budget;
+} mp_adjoint_config;
 
 typedef struct mp_ctx mp_ctx;
 
@@ -295,6 +330,24 @@ long long mp_launch_count(mp_ctx *ctx);
  * the per-kernel roofline; no counterpart in MPulse. */
 int mp_kernel_times(mp_ctx *ctx, int n_steps, double *e_half_ms, double *b_half_ms,
                     double *sources_ms);
+
+/* Runs adj->steps steps like mp_step and returns the objective J of adj over
+ * them in *J (FP64 accumulation).  No counterpart in MPulse. */
+int mp_objective(mp_ctx *ctx, const mp_adjoint_config *adj, double *J);
+
+/* Like mp_objective, then the gradient of J with respect to the design
+ * parameters by the discrete adjoint of the steps run: the transposed curls,
+ * the reverse CPML and PLRC recursions and the linearised Kerr solve, run
+ * backwards over the steps, with the forward recomputed segment by segment
+ * from checkpoints (mp_adjoint_config).  grad_eps, grad_deps_scale and
+ * grad_chi_scale receive dJ/d DesignEps, dJ/d DesignDepsScale and
+ * dJ/d DesignChiScale per design cell (host arrays of the design box's size,
+ * x fastest; NULL skips one).  The state ends as after mp_objective.  Needs a
+ * PLRC solver, the xy-periodic boundary, the global-load staging and a
+ * non-empty design box; the sources must not depend on the design (they do
+ * not).  No counterpart in MPulse. */
+int mp_adjoint(mp_ctx *ctx, const mp_adjoint_config *adj, double *J, double *grad_eps,
+               double *grad_deps_scale, double *grad_chi_scale);
 
 /* Copies the message of the last failure (or "") into buf. */
 int mp_last_error(mp_ctx *ctx, char *buf, size_t n);

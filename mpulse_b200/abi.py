@@ -41,7 +41,10 @@ MP_STAGING_AUTO, MP_STAGING_GLOBAL, MP_STAGING_TMA = 0, 1, 2
 (MP_SOURCE_NONE, MP_SOURCE_PLANE_WAVE, MP_SOURCE_PLANE_GAUSS,
  MP_SOURCE_SHORT_PULSE, MP_SOURCE_FOCUSED_PULSE, MP_SOURCE_GAUSS_BEAM) = range(6)
 
+MP_OBJ_E2_BOX, MP_OBJ_SZ_PLANE = 1, 2
+
 FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz")
+DESIGN_NAMES = ("DesignEps", "DesignDepsScale", "DesignChiScale")
 PSI_NAMES = tuple(f"Psi{ri}{n}{c}" for ri in "RI" for n in (1, 2, 3) for c in "xyz")
 
 
@@ -106,6 +109,7 @@ class Config(C.Structure):
         ("newton_tol", C.c_double),
         ("staging", C.c_int),
         ("device", C.c_int),
+        ("design_box", C.c_int * 6),
     ]
 
     def field_count(self) -> int:
@@ -114,6 +118,34 @@ class Config(C.Structure):
 
     def field_shape(self):
         return (self.nz + 2, self.ny, self.nx)
+
+
+class AdjointConfig(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("box", C.c_int * 6),
+        ("steps", C.c_int),
+        ("checkpoint_every", C.c_int),
+        ("mem_budget", C.c_double),
+    ]
+
+
+def adjoint_config(kind: int, box, steps: int, checkpoint_every: int = 0, mem_budget: float = 0.0) -> AdjointConfig:
+    a = AdjointConfig()
+    a.kind = kind
+    a.box[:] = tuple(box)
+    a.steps = steps
+    a.checkpoint_every = checkpoint_every
+    a.mem_budget = mem_budget
+    return a
+
+
+def design_shape(c: Config):
+    """(nz, ny, nx) extent of the design box, or None when it is empty."""
+    b = c.design_box
+    if b[0] > b[1]:
+        return None
+    return (b[5] - b[4] + 1, b[3] - b[2] + 1, b[1] - b[0] + 1)
 
 
 def default_source(kind: int = MP_SOURCE_NONE) -> Source:
@@ -171,6 +203,7 @@ def default_config() -> Config:
     c.newton_tol = 1e-9
     c.staging = MP_STAGING_AUTO
     c.device = 0
+    c.design_box[:] = (1, 0, 1, 0, 1, 0)
     return c
 
 

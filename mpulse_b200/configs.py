@@ -195,3 +195,47 @@ def c1_initial_fields(cfg: abi.Config) -> dict:
     k0 = 2 * math.pi / 0.8
     z0 = field_fwhm_to_t0(5.0)  # spatial 1/e half-width = c t0
     return pulse_init_fields(cfg, k=k0, z0=z0, zc=20 * cfg.dz)
+
+
+def c4_adjoint(precision=abi.MP_FP64, n=96, seed=0) -> tuple:
+    """Adjoint-gradient workload, 96^3 (dt = MEDIUM_COURANT dx / c), 10-cell
+    CPML on all faces, linear single-pole Lorentz medium (Delta eps = 0.5,
+    lambda_res = 100 nm, gamma = 1e-3 omega_res) everywhere, a 32^3 design
+    region at the centre whose eps_inf is drawn i.i.d. uniform in [1, 4] from
+    torch.Generator().manual_seed(seed), an Ex plane-wave pulse (lambda0 =
+    800 nm, 10 fs FWHM) injected at z = 14, and the objective
+    J = sum_t sum |E|^2 dt over the 8^3 monitor box centred at (48, 48, 80),
+    1500 steps with a checkpoint every 50.
+    Returns (config, {design map name: array}, adjoint config)."""
+    import torch
+
+    c = base(n, n, n, courant=MEDIUM_COURANT)
+    c.precision = precision
+    c.solver = abi.MP_SOLVER_PLRC_LIN
+    c.boundary = abi.MP_BOUNDARY_XY_PERIODIC
+    _set_poles(c, (lorentz_pole(0.5, 0.1),))
+    c.eps = 1.0
+    c.medium_z0, c.medium_z1 = 0, n + 1
+    c.cpml = abi.MP_CPML_ALL
+    c.cpml_d = 10
+    c.cpml_kappa_max = 1.0
+    c.cpml_a_max = 0.0
+    c.cpml_sigma_max = sigma_max_for(1e-6, 10, c.dz)
+    k0 = 2 * math.pi / 0.8
+    width = k0 * field_fwhm_to_t0(10.0)
+    c.n_sources = 1
+    s = c.sources[0]
+    s.kind = abi.MP_SOURCE_PLANE_GAUSS
+    s.distance = 14
+    s.k[:] = (0.0, 0.0, k0)
+    s.H[:] = (0.0, 1.0, 0.0)
+    s.width = width
+    s.offset = 3.0 * width
+    s.eps = 1.0
+    lo, hi = n // 2 - 15, n // 2 + 16          # 32 cells centred on n/2 + 1/2
+    c.design_box[:] = (lo, hi, lo, hi, lo, hi)
+    g = torch.Generator().manual_seed(seed)
+    eps = 1.0 + 3.0 * torch.rand((32, 32, 32), generator=g, dtype=torch.float64)
+    m = n // 2
+    adj = abi.adjoint_config(abi.MP_OBJ_E2_BOX, (m - 3, m + 4, m - 3, m + 4, 77, 84), 1500, checkpoint_every=50)
+    return c, {"DesignEps": eps.numpy()}, adj

@@ -41,6 +41,13 @@ cudaError_t launch_e_half_tma(const EParams<T> &, const ETmaMaps &, int, int, cu
 template <typename T>
 cudaError_t launch_b_half_tma(const BParams<T> &, const BTmaMaps &, cudaStream_t);
 void tma_boxes(int esz, int e_box[7][2], int b_box[6][2]);
+template <typename T> cudaError_t launch_adj_e(const AdjParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_adj_b(const AdjParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_adj_init(const AdjParams<T> &, cudaStream_t);
+template <typename T>
+cudaError_t launch_objective_term(const T *const E[3], const T *const B[3], int nx, int ny, long long plane, int kind,
+                                  const int box0[6], double f, double *out, cudaStream_t st);
+cudaError_t launch_sum_terms(const double *terms, long long n, double *out, cudaStream_t st);
 }  // namespace mpb
 
 using namespace mpb;
@@ -105,6 +112,14 @@ struct mp_ctx {
   bool tma = false;  // TMA-staged kernels in use
   ETmaMaps etma;
   BTmaMaps btma;
+  // design region (mp_config.design_box): FP64 maps eps, Delta-eps factor, chi factor
+  bool design = false;
+  size_t dcells = 0;
+  double *d_design[3] = {nullptr, nullptr, nullptr};
+  DesignParams dp;
+  // FP64 PLRC constants of the active poles: [D, dxi0, Crec][slot][re, im]
+  double coef[3][3][2] = {{{0}}};
+  double sumChi0 = 0, sumXi0 = 0;
   std::vector<void *> allocs;
 };
 
@@ -211,6 +226,18 @@ int validate(const mp_config *c) {
   if (c->newton_max_iter < 1) return set_err(nullptr, MP_ERR_INVALID, "newton_max_iter must be >= 1");
   if (c->staging != MP_STAGING_AUTO && c->staging != MP_STAGING_GLOBAL && c->staging != MP_STAGING_TMA)
     return set_err(nullptr, MP_ERR_INVALID, "unknown staging %d", c->staging);
+  const int *db = c->design_box;
+  if (db[0] <= db[1]) {
+    if (!plrc) return set_err(nullptr, MP_ERR_INVALID, "a design region needs a PLRC solver");
+    if (db[0] < 1 || db[1] > c->nx || db[2] < 1 || db[2] > db[3] || db[3] > c->ny || db[4] < 1 || db[4] > db[5] ||
+        db[5] > c->nz)
+      return set_err(nullptr, MP_ERR_INVALID, "design box outside the interior");
+    if (db[4] < c->medium_z0 || db[5] > c->medium_z1)
+      return set_err(nullptr, MP_ERR_INVALID, "design box outside the medium planes %d..%d", c->medium_z0,
+                     c->medium_z1);
+    if (c->staging == MP_STAGING_TMA)
+      return set_err(nullptr, MP_ERR_UNSUPPORTED, "design regions use the global-load kernels (staging GLOBAL/AUTO)");
+  }
   if (c->staging == MP_STAGING_TMA && (c->nx % kTmaTileX != 0 || c->ny % kTmaTileY != 0))
     return set_err(nullptr, MP_ERR_UNSUPPORTED, "TMA staging needs nx a multiple of %d and ny of %d", kTmaTileX,
                    kTmaTileY);
@@ -284,6 +311,8 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
     fill_face(ep.cpml[f], c->cpE[f], lines);
     fill_face(bp.cpml[f], c->cpH[f], lines);
   }
+  ep.design.x0 = 1;  // none; set by create_impl when the config has a design box
+  ep.design.x1 = 0;
   ep.n_src = bp.n_src = c->nsrc;
   ep.src_mult = bp.src_mult = c->src_mult;
   const size_t pl = size_t(c->plane);
@@ -433,6 +462,11 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
       }
     }
     const double sumChi0 = sumChi.real(), sumXi0 = sumXi.real();
+    c->sumChi0 = sumChi0;
+    c->sumXi0 = sumXi0;
+    for (int a = 0; a < 3; ++a)
+      for (int s = 0; s < 3; ++s)
+        for (int r = 0; r < 2; ++r) c->coef[a][s][r] = coef[a][s][r];
     numer = g.eps - sumXi0 - 0.0;
     denom = (c->mode == MODE_PLRC_LIN) ? g.eps + (sumChi0 - sumXi0) + 0.0 : g.eps + sumChi0 - sumXi0 + 0.0;
     if (c->mz0 <= c->mz1) {
@@ -632,6 +666,41 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
 
   if (c->fp32) build_params<float>(c, c->epf, c->bpf, ikE_off, ikH_off, bzy_off, coef, numer, denom);
   else build_params<double>(c, c->epd, c->bpd, ikE_off, ikH_off, bzy_off, coef, numer, denom);
+
+  // design region: FP64 maps with the defaults eps, 1, 1
+  if (g.design_box[0] <= g.design_box[1]) {
+    const int *db = g.design_box;
+    DesignParams &d = c->dp;
+    d.x0 = db[0] - 1; d.x1 = db[1] - 1;
+    d.y0 = db[2] - 1; d.y1 = db[3] - 1;
+    d.z0 = db[4]; d.z1 = db[5];
+    d.bx = db[1] - db[0] + 1;
+    d.by = db[3] - db[2] + 1;
+    c->dcells = size_t(d.bx) * d.by * (db[5] - db[4] + 1);
+    const double init[3] = {g.eps, 1.0, 1.0};
+    for (int a = 0; a < 3; ++a) {
+      MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_design[a]), c->dcells * sizeof(double)), "design allocation");
+      std::vector<double> h(c->dcells, init[a]);
+      MPB_TRY(cudaMemcpyAsync(c->d_design[a], h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+              "cudaMemcpy");
+      MPB_TRY(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    }
+    d.eps = c->d_design[0];
+    d.dscale = c->d_design[1];
+    d.chiscale = c->d_design[2];
+    for (int s = 0; s < 3; ++s)
+      for (int r = 0; r < 2; ++r) {
+        d.pD[s][r] = coef[0][s][r];
+        d.pxi[s][r] = coef[1][s][r];
+      }
+    d.sumChi0 = c->sumChi0;
+    d.sumXi0 = c->sumXi0;
+    d.chi = g.chi;
+    d.lin = c->mode == MODE_PLRC_LIN;
+    c->design = true;
+    if (c->fp32) c->epf.design = d;
+    else c->epd.design = d;
+  }
   // AUTO = GLOBAL: on the 256x256x512 PLRC + Kerr workload the global-load
   // kernels (E 0.92 ms, B 0.47 ms per launch) beat the TMA-staged ones
   // (E 1.12 ms, B 0.61 ms), whose 12 small tile copies per plane and block
@@ -787,6 +856,15 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
   return MP_OK;
 }
 
+// "DesignEps", "DesignDepsScale", "DesignChiScale": index of the map, or -1
+int design_map(const mp_ctx *c, const char *name) {
+  if (!c->design || !name) return -1;
+  static const char *dn[3] = {"DesignEps", "DesignDepsScale", "DesignChiScale"};
+  for (int a = 0; a < 3; ++a)
+    if (!strcmp(name, dn[a])) return a;
+  return -1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -837,6 +915,7 @@ void mp_config_defaults(mp_config *c) {
   c->newton_max_iter = 64;
   c->newton_tol = 1e-9;       // fdtd_plrc.cpp:414
   c->device = 0;
+  c->design_box[0] = c->design_box[2] = c->design_box[4] = 1;  // empty: x0 > x1
 }
 
 int mp_create(const mp_config *cfg, mp_ctx **out) {
@@ -874,6 +953,10 @@ int mp_set_stream(mp_ctx *c, void *s) {
 
 int mp_field_size(mp_ctx *c, const char *name, size_t *count) {
   if (!c || !count) return MP_ERR_INVALID;
+  if (design_map(c, name) >= 0) {
+    *count = c->dcells;
+    return MP_OK;
+  }
   FieldView v;
   int rc = resolve(c, name, v);
   if (rc != MP_OK) return rc;
@@ -883,6 +966,14 @@ int mp_field_size(mp_ctx *c, const char *name, size_t *count) {
 
 int mp_upload(mp_ctx *c, const char *name, const double *host, size_t count) {
   if (!c || !host) return MP_ERR_INVALID;
+  const int dm = design_map(c, name);
+  if (dm >= 0) {
+    if (count != c->dcells) return set_err(c, MP_ERR_INVALID, "%s: %zu values, expected %zu", name, count, c->dcells);
+    cudaSetDevice(c->cfg.device);
+    cudaError_t e = cudaMemcpyAsync(c->d_design[dm], host, count * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? MP_OK : cuda_err(c, e, "design upload");
+  }
   FieldView v;
   int rc = resolve(c, name, v);
   if (rc != MP_OK) return rc;
@@ -912,6 +1003,14 @@ int mp_upload(mp_ctx *c, const char *name, const double *host, size_t count) {
 
 int mp_download(mp_ctx *c, const char *name, double *host, size_t count) {
   if (!c || !host) return MP_ERR_INVALID;
+  const int dm = design_map(c, name);
+  if (dm >= 0) {
+    if (count != c->dcells) return set_err(c, MP_ERR_INVALID, "%s: %zu values, expected %zu", name, count, c->dcells);
+    cudaSetDevice(c->cfg.device);
+    cudaError_t e = cudaMemcpyAsync(host, c->d_design[dm], count * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? MP_OK : cuda_err(c, e, "design download");
+  }
   FieldView v;
   int rc = resolve(c, name, v);
   if (rc != MP_OK) return rc;
@@ -1059,6 +1158,332 @@ int mp_last_error(mp_ctx *c, char *buf, size_t n) {
   const char *m = c ? c->err.c_str() : g_create_err;
   snprintf(buf, n, "%s", m);
   return MP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// mp_objective / mp_adjoint
+
+namespace {
+
+// Device buffers of one call, freed (after the stream drains) when it returns.
+struct DevBufs {
+  cudaStream_t st;
+  std::vector<void *> p;
+  explicit DevBufs(cudaStream_t s) : st(s) {}
+  ~DevBufs() {
+    cudaStreamSynchronize(st);
+    for (void *q : p) cudaFree(q);
+  }
+  cudaError_t alloc(void **out, size_t bytes) {
+    *out = nullptr;
+    if (!bytes) return cudaSuccess;
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e != cudaSuccess) return e;
+    p.push_back(*out);
+    return cudaMemsetAsync(*out, 0, bytes, st);
+  }
+};
+
+// The arrays that make up the forward state: fields, PLRC accumulators, CPML psi.
+std::vector<std::pair<void *, size_t>> state_regions(const mp_ctx *c) {
+  std::vector<std::pair<void *, size_t>> r;
+  for (int f = 0; f < 6; ++f) r.emplace_back(c->F[f], c->fcount * c->esz);
+  for (int s = 0; s < c->np; ++s)
+    for (int a = 0; a < 3; ++a) r.emplace_back(c->psi[s][a], 2 * c->psi_cells * c->esz);
+  for (int f = 0; f < 6; ++f)
+    for (const LayerHost *L : {&c->cpE[f], &c->cpH[f]})
+      if (L->active) {
+        r.emplace_back(L->psi0, L->n * c->esz);
+        r.emplace_back(L->psi1, L->n * c->esz);
+      }
+  return r;
+}
+
+int check_objective(mp_ctx *c, const mp_adjoint_config *a) {
+  const mp_config &g = c->cfg;
+  if (a->kind != MP_OBJ_E2_BOX && a->kind != MP_OBJ_SZ_PLANE)
+    return set_err(c, MP_ERR_INVALID, "unknown objective kind %d", a->kind);
+  if (a->steps < 1) return set_err(c, MP_ERR_INVALID, "steps must be >= 1");
+  const int *b = a->box;
+  if (b[0] < 1 || b[0] > b[1] || b[1] > g.nx || b[2] < 1 || b[2] > b[3] || b[3] > g.ny || b[4] < 1 || b[4] > b[5] ||
+      b[5] > g.nz)
+    return set_err(c, MP_ERR_INVALID, "objective box outside the interior");
+  return MP_OK;
+}
+
+// 0-based x/y, MPulse z box of the objective (the Sz plane is box[4])
+void objective_box(const mp_adjoint_config *a, int b0[6]) {
+  b0[0] = a->box[0] - 1;
+  b0[1] = a->box[1] - 1;
+  b0[2] = a->box[2] - 1;
+  b0[3] = a->box[3] - 1;
+  b0[4] = a->box[4];
+  b0[5] = a->kind == MP_OBJ_E2_BOX ? a->box[5] : a->box[4];
+}
+
+template <typename T>
+int objective_term(mp_ctx *c, const mp_adjoint_config *a, double *out) {
+  const mp_config &g = c->cfg;
+  const T *E[3] = {static_cast<const T *>(c->F[0]), static_cast<const T *>(c->F[1]), static_cast<const T *>(c->F[2])};
+  const T *B[3] = {static_cast<const T *>(c->F[3]), static_cast<const T *>(c->F[4]), static_cast<const T *>(c->F[5])};
+  int b0[6];
+  objective_box(a, b0);
+  const double f = a->kind == MP_OBJ_E2_BOX ? g.dt : g.dt * g.dx * g.dy;
+  cudaError_t e = launch_objective_term<T>(E, B, g.nx, g.ny, c->plane, a->kind, b0, f, out, c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "objective kernel");
+  c->launches++;
+  return MP_OK;
+}
+
+int read_sum(mp_ctx *c, double *terms, long long n, double *J) {
+  cudaError_t e = launch_sum_terms(terms, n, terms + n, c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "sum kernel");
+  c->launches++;
+  e = cudaMemcpyAsync(c->h_diag, terms + n, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "objective read");
+  *J = *c->h_diag;
+  return MP_OK;
+}
+
+template <typename T>
+int objective_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_config *a, double *J) {
+  DevBufs buf(c->stream);
+  double *terms;
+  cudaError_t e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(a->steps) + 1) * sizeof(double));
+  if (e != cudaSuccess) return cuda_err(c, e, "objective allocation");
+  for (long long n = 0; n < a->steps; ++n) {
+    int rc = step_impl<T>(c, ep, bp, 1);
+    if (rc == MP_OK) rc = objective_term<T>(c, a, terms + n);
+    if (rc != MP_OK) return rc;
+  }
+  const int rc = read_sum(c, terms, a->steps, J);
+  return rc != MP_OK ? rc : mp_check_status(c);
+}
+
+// Forward with checkpoints, then the reverse pass segment by segment: a
+// segment [n0, n1) is recomputed from its checkpoint keeping E (and, for the Sz
+// objective, Bx and By on the plane) of every state n0..n1, then stepped back
+// with adj_e / adj_b from n1 - 1 down to n0.  The last segment's history is
+// kept during the first forward run, so with one segment nothing is
+// recomputed.
+template <typename T>
+int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_config *a, double *J, double *gout[3]) {
+  const mp_config &g = c->cfg;
+  const long long Tn = a->steps;
+  const auto regions = state_regions(c);
+  size_t S = 0;
+  for (const auto &r : regions) S += r.second;
+  const bool sz = a->kind == MP_OBJ_SZ_PLANE;
+  const size_t fbytes = c->fcount * sizeof(T), pbytes = size_t(c->plane) * sizeof(T);
+  const size_t H = 3 * fbytes + (sz ? 2 * pbytes : 0);
+  long long K = a->checkpoint_every;
+  if (K <= 0) {
+    if (!(a->mem_budget > 0)) {
+      K = Tn;
+    } else {
+      K = 0;
+      for (long long k = Tn; k >= 1 && !K; --k) {
+        const long long nseg = (Tn + k - 1) / k;
+        if (double(nseg + 1) * double(S) + double(k + 1) * double(H) <= a->mem_budget) K = k;
+      }
+      if (!K)
+        return set_err(c, MP_ERR_NO_MEMORY,
+                       "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
+                       a->mem_budget, S, H);
+    }
+  }
+  K = std::min(K, Tn);
+  const long long nseg = (Tn + K - 1) / K, last0 = (nseg - 1) * K;
+
+  DevBufs buf(c->stream);
+  cudaError_t e;
+  char *ckpt, *hist;
+  double *terms;
+  if ((e = buf.alloc(reinterpret_cast<void **>(&ckpt), size_t(nseg + 1) * S)) != cudaSuccess ||
+      (e = buf.alloc(reinterpret_cast<void **>(&hist), size_t(K + 1) * H)) != cudaSuccess ||
+      (e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(Tn) + 1) * sizeof(double))) != cudaSuccess)
+    return cuda_err(c, e, "checkpoint allocation");
+  AdjParams<T> p = AdjParams<T>();
+  for (int q = 0; q < 3; ++q) {
+    void *eb, *bb, *gg;
+    double *gr;
+    if ((e = buf.alloc(&eb, fbytes)) != cudaSuccess || (e = buf.alloc(&bb, fbytes)) != cudaSuccess ||
+        (e = buf.alloc(&gg, fbytes)) != cudaSuccess ||
+        (e = buf.alloc(reinterpret_cast<void **>(&gr), c->dcells * sizeof(double))) != cudaSuccess)
+      return cuda_err(c, e, "adjoint allocation");
+    p.Eb[q] = static_cast<T *>(eb);
+    p.Bb[q] = static_cast<T *>(bb);
+    p.G[q] = static_cast<T *>(gg);
+    p.grad[q] = gr;
+  }
+  for (int s = 0; s < c->np; ++s)
+    for (int q = 0; q < 3; ++q) {
+      void *ps;
+      if ((e = buf.alloc(&ps, 2 * c->psi_cells * sizeof(T))) != cudaSuccess) return cuda_err(c, e, "adjoint allocation");
+      p.psib[s][q] = static_cast<T *>(ps);
+    }
+  for (int f = 0; f < 6; ++f)
+    for (int isH = 0; isH < 2; ++isH) {
+      const LayerHost &L = isH ? c->cpH[f] : c->cpE[f];
+      const CpmlFace<T> &F = isH ? bp.cpml[f] : ep.cpml[f];
+      AdjFace<T> &A = isH ? p.fh[f] : p.fe[f];
+      A.active = L.active;
+      if (!L.active) continue;
+      A.dim = L.dim; A.lo = L.lo; A.hi = L.hi; A.zlo = L.zlo; A.ex = L.ex; A.ey = L.ey;
+      A.b = F.b;
+      A.c = F.c;
+      void *a0, *a1;
+      if ((e = buf.alloc(&a0, L.n * sizeof(T))) != cudaSuccess || (e = buf.alloc(&a1, L.n * sizeof(T))) != cudaSuccess)
+        return cuda_err(c, e, "adjoint allocation");
+      A.a0 = static_cast<T *>(a0);
+      A.a1 = static_cast<T *>(a1);
+    }
+  p.nx = g.nx; p.ny = g.ny; p.nz = g.nz;
+  p.plane = c->plane;
+  p.dt = g.dt;
+  for (int q = 0; q < 3; ++q) {
+    p.ikE[q] = ep.ik[q];
+    p.ikH[q] = bp.ik[q];
+  }
+  p.ikH_bzy = bp.ik_bz_y;
+  for (int s = 0; s < 3; ++s)
+    for (int r = 0; r < 2; ++r) {
+      p.pD[s][r] = c->coef[0][s][r];
+      p.pxi[s][r] = c->coef[1][s][r];
+      p.pC[s][r] = c->coef[2][s][r];
+    }
+  p.sumChi0 = c->sumChi0;
+  p.sumXi0 = c->sumXi0;
+  p.chi = g.chi;
+  p.eps = g.eps;
+  p.eps_bg = g.eps_bg;
+  p.np = c->np;
+  p.mz0 = c->mz0;
+  p.mz1 = c->mz1;
+  p.nonlin = c->mode == MODE_PLRC_NONLIN;
+  p.design = c->dp;
+  p.obj_kind = a->kind;
+  int b0[6];
+  objective_box(a, b0);
+  p.ox0 = b0[0]; p.ox1 = b0[1]; p.oy0 = b0[2]; p.oy1 = b0[3]; p.oz0 = b0[4]; p.oz1 = b0[5];
+  p.obj_f = a->kind == MP_OBJ_E2_BOX ? 2.0 * g.dt : g.dt * g.dx * g.dy;
+
+  auto copy_state = [&](long long slot, bool save) -> cudaError_t {
+    size_t off = 0;
+    for (const auto &r : regions) {
+      char *ck = ckpt + size_t(slot) * S + off;
+      cudaError_t err = save ? cudaMemcpyAsync(ck, r.first, r.second, cudaMemcpyDeviceToDevice, c->stream)
+                             : cudaMemcpyAsync(r.first, ck, r.second, cudaMemcpyDeviceToDevice, c->stream);
+      if (err != cudaSuccess) return err;
+      off += r.second;
+    }
+    return cudaSuccess;
+  };
+  auto record = [&](long long slot) -> cudaError_t {
+    char *h = hist + size_t(slot) * H;
+    for (int q = 0; q < 3; ++q) {
+      cudaError_t err = cudaMemcpyAsync(h + q * fbytes, c->F[q], fbytes, cudaMemcpyDeviceToDevice, c->stream);
+      if (err != cudaSuccess) return err;
+    }
+    if (sz)
+      for (int q = 0; q < 2; ++q) {
+        const char *src = static_cast<const char *>(c->F[3 + q]) + size_t(b0[4]) * pbytes;
+        cudaError_t err = cudaMemcpyAsync(h + 3 * fbytes + q * pbytes, src, pbytes, cudaMemcpyDeviceToDevice, c->stream);
+        if (err != cudaSuccess) return err;
+      }
+    return cudaSuccess;
+  };
+  auto slot_e = [&](long long slot, int q) {
+    return reinterpret_cast<const T *>(hist + size_t(slot) * H + q * fbytes);
+  };
+  auto slot_b = [&](long long slot, int q) {
+    return sz ? reinterpret_cast<const T *>(hist + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
+  };
+
+  // ---- forward
+  const long long t0 = c->time;
+  for (long long n = 0; n < Tn; ++n) {
+    if (n % K == 0 && (e = copy_state(n / K, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+    if (n >= last0 && (e = record(n - last0)) != cudaSuccess) return cuda_err(c, e, "history copy");
+    int rc = step_impl<T>(c, ep, bp, 1);
+    if (rc == MP_OK) rc = objective_term<T>(c, a, terms + n);
+    if (rc != MP_OK) return rc;
+  }
+  if ((e = record(Tn - last0)) != cudaSuccess || (e = copy_state(nseg, true)) != cudaSuccess)
+    return cuda_err(c, e, "checkpoint copy");
+  int rc = read_sum(c, terms, Tn, J);
+  if (rc == MP_OK) rc = mp_check_status(c);
+  if (rc != MP_OK) return rc;
+
+  // ---- reverse
+  for (int q = 0; q < 3; ++q) p.En[q] = slot_e(Tn - last0, q);
+  p.obx = slot_b(Tn - last0, 0);
+  p.oby = slot_b(Tn - last0, 1);
+  if ((e = launch_adj_init<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint init kernel");
+  c->launches++;
+  for (long long m = nseg - 1; m >= 0; --m) {
+    const long long n0 = m * K, n1 = std::min(n0 + K, Tn);
+    if (m != nseg - 1) {
+      if ((e = copy_state(m, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
+      c->time = t0 + n0;
+      for (long long n = n0; n < n1; ++n) {
+        if ((e = record(n - n0)) != cudaSuccess) return cuda_err(c, e, "history copy");
+        if ((rc = step_impl<T>(c, ep, bp, 1)) != MP_OK) return rc;
+      }
+      if ((e = record(n1 - n0)) != cudaSuccess) return cuda_err(c, e, "history copy");
+    }
+    for (long long n = n1 - 1; n >= n0; --n) {
+      for (int q = 0; q < 3; ++q) {
+        p.En[q] = slot_e(n - n0, q);
+        p.En1[q] = slot_e(n - n0 + 1, q);
+      }
+      p.obx = slot_b(n - n0, 0);
+      p.oby = slot_b(n - n0, 1);
+      p.add_obj = n >= 1;
+      if ((e = launch_adj_e<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint E kernel");
+      if ((e = launch_adj_b<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint B kernel");
+      c->launches += 2;
+    }
+  }
+  if ((e = copy_state(nseg, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
+  c->time = t0 + Tn;
+  for (int q = 0; q < 3; ++q)
+    if (gout[q] && (e = cudaMemcpyAsync(gout[q], p.grad[q], c->dcells * sizeof(double), cudaMemcpyDeviceToHost,
+                                        c->stream)) != cudaSuccess)
+      return cuda_err(c, e, "gradient read");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint");
+  return mp_check_status(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_objective(mp_ctx *c, const mp_adjoint_config *a, double *J) {
+  if (!c || !a || !J) return MP_ERR_INVALID;
+  int rc = check_objective(c, a);
+  if (rc != MP_OK) return rc;
+  cudaSetDevice(c->cfg.device);
+  return c->fp32 ? objective_impl<float>(c, c->epf, c->bpf, a, J) : objective_impl<double>(c, c->epd, c->bpd, a, J);
+}
+
+int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_eps, double *grad_deps_scale,
+               double *grad_chi_scale) {
+  if (!c || !a || !J) return MP_ERR_INVALID;
+  int rc = check_objective(c, a);
+  if (rc != MP_OK) return rc;
+  if (c->mode != MODE_PLRC_LIN && c->mode != MODE_PLRC_NONLIN)
+    return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint needs a PLRC solver");
+  if (c->cfg.boundary != MP_BOUNDARY_XY_PERIODIC)
+    return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint needs the xy-periodic boundary");
+  if (!c->design) return set_err(c, MP_ERR_INVALID, "mp_adjoint needs a design region (mp_config.design_box)");
+  if (c->tma) return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint uses the global-load kernels");
+  cudaSetDevice(c->cfg.device);
+  double *g[3] = {grad_eps, grad_deps_scale, grad_chi_scale};
+  return c->fp32 ? adjoint_impl<float>(c, c->epf, c->bpf, a, J, g) : adjoint_impl<double>(c, c->epd, c->bpd, a, J, g);
 }
 
 }  // extern "C"

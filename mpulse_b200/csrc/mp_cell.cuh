@@ -82,12 +82,59 @@ struct BIn {
 // (fdtd_plain.cpp:37-77) or FDTD_Nonlinear::stepD (fdtd_nl.cpp:38-100).
 // i, j are 0-based interior indices (MPulse i+1, j+1); k is MPulse's z index.
 // q holds the cell's PLRC accumulators on entry and their new values on exit.
-template <typename T, int MODE, int NP>
+// The medium coefficients of one cell: the kernel parameters, or for a cell of
+// the design region the same formulas with its eps_infinity, Delta-eps factor s
+// and chi factor u (FP64, then rounded to T like the host's).  Factors 1 and
+// eps_infinity = eps reproduce the kernel parameters bit for bit.
+template <typename T, int NP>
+struct CellCoef {
+  T numer, inv_denom, chi;
+  double chi_over_denom;
+  T pD[NP > 0 ? NP : 1][2], pxi[NP > 0 ? NP : 1][2];
+};
+
+template <typename T, int NP, bool DESIGN>
+__device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int k, bool med, CellCoef<T, NP> &cc) {
+  cc.numer = p.numer;
+  cc.inv_denom = p.inv_denom;
+  cc.chi = p.chi;
+  cc.chi_over_denom = p.chi_over_denom;
+#pragma unroll
+  for (int n = 0; n < (NP > 0 ? NP : 1); ++n)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      cc.pD[n][r] = p.pD[n][r];
+      cc.pxi[n][r] = p.pxi[n][r];
+    }
+  if (DESIGN) {
+    const DesignParams &d = p.design;
+    if (med && i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1 && k >= d.z0 && k <= d.z1) {
+      const long long di = ((long long)(k - d.z0) * d.by + (j - d.y0)) * d.bx + (i - d.x0);
+      const double e = d.eps[di], s = d.dscale[di], u = d.chiscale[di];
+      const double denom = d.lin ? e + s * (d.sumChi0 - d.sumXi0) : e + s * d.sumChi0 - s * d.sumXi0;
+      cc.numer = T(e - s * d.sumXi0);
+      cc.inv_denom = T(1.0 / denom);
+      cc.chi = T(u * d.chi);
+      cc.chi_over_denom = u * d.chi / denom;
+#pragma unroll
+      for (int n = 0; n < NP; ++n)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          cc.pD[n][r] = T(s * d.pD[n][r]);
+          cc.pxi[n][r] = T(s * d.pxi[n][r]);
+        }
+    }
+  }
+}
+
+template <typename T, int MODE, int NP, bool DESIGN = false>
 __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
                                        const EIn<T> &v, T ikx, T iky, T ikz,
                                        typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
                                        T &ezn) {
   const T dt = p.dt;
+  CellCoef<T, NP> lc;
+  cell_coef<T, NP, DESIGN>(p, i, j, k, med, lc);
   // ---- loads of the CPML psi of the faces containing the cell, and of the
   // injection plane
   T cp0[6], cp1[6], cb[6], cc[6];
@@ -181,12 +228,12 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           // psi~ = (dchi0 - dxi0) e + psi ; Psi += Re psi~
-          const T ar = p.pD[n][0] * e3[c] + q[n][c].x;
-          const T ai = p.pD[n][1] * e3[c] + q[n][c].y;
+          const T ar = lc.pD[n][0] * e3[c] + q[n][c].x;
+          const T ai = lc.pD[n][1] * e3[c] + q[n][c].y;
           P3[c] += ar;
           // psi <- dxi0 e + Crec psi~
-          q[n][c].x = p.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
-          q[n][c].y = p.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
+          q[n][c].x = lc.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
+          q[n][c].y = lc.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
         }
       }
       Px = P3[0];
@@ -194,18 +241,18 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       Pz = P3[2];
     }
     if (MODE == MODE_PLRC_LIN) {
-      exn = (p.numer * ex + (dt * (cbx + jx) + Px)) * p.inv_denom;
-      eyn = (p.numer * ey + (dt * (cby + jy) + Py)) * p.inv_denom;
-      ezn = (p.numer * ez + (dt * (cbz + jz) + Pz)) * p.inv_denom;
+      exn = (lc.numer * ex + (dt * (cbx + jx) + Px)) * lc.inv_denom;
+      eyn = (lc.numer * ey + (dt * (cby + jy) + Py)) * lc.inv_denom;
+      ezn = (lc.numer * ez + (dt * (cbz + jz) + Pz)) * lc.inv_denom;
     } else {
       const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
-      const T f = p.numer + p.chi * T(E2);
-      const T cx = (f * ex + dt * (cbx + jx) + Px) * p.inv_denom;
-      const T cy = (f * ey + dt * (cby + jy) + Py) * p.inv_denom;
-      const T cz = (f * ez + dt * (cbz + jz) + Pz) * p.inv_denom;
+      const T f = lc.numer + lc.chi * T(E2);
+      const T cx = (f * ex + dt * (cbx + jx) + Px) * lc.inv_denom;
+      const T cy = (f * ey + dt * (cby + jy) + Py) * lc.inv_denom;
+      const T cz = (f * ez + dt * (cbz + jz) + Pz) * lc.inv_denom;
       const double C = sqrt((double)cx * cx + (double)cy * cy + (double)cz * cz);
       if (C > 0) {
-        const double E = kerr_newton(sqrt(E2), p.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
+        const double E = kerr_newton(sqrt(E2), lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
         exn = T(E * cx / C);
         eyn = T(E * cy / C);
         ezn = T(E * cz / C);

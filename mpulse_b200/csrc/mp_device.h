@@ -63,6 +63,18 @@ struct SourcePlane {
   const T *v1;      // component transverse2 (y)
 };
 
+// Per-cell design parameters (mp_config.design_box): eps_infinity, a factor
+// on every pole's Delta epsilon and a factor on chi, box-sized FP64 maps with x
+// fastest.  x0..x1, y0..y1 are 0-based interior indices, z0..z1 MPulse planes.
+struct DesignParams {
+  int x0, x1, y0, y1, z0, z1;  // inclusive; x0 > x1: no design region
+  int bx, by;                  // box extents in x and y
+  const double *eps, *dscale, *chiscale;
+  double pD[3][2], pxi[3][2];  // dchi0 - dxi0 and dxi0 of the active poles, FP64
+  double sumChi0, sumXi0, chi;
+  int lin;                     // PLRC_LIN: denominator eps + (sumChi0 - sumXi0)
+};
+
 template <typename T>
 struct EParams {
   int nx, ny, nz;
@@ -92,6 +104,7 @@ struct EParams {
   const T *ik[3];         // 1 / (kappa_E * d) per index, per axis
 
   CpmlFace<T> cpml[6];    // E-side CPML currents in MPulse's current order
+  DesignParams design;
   int n_src;
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
@@ -115,6 +128,44 @@ struct BParams {
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
   int *status;
+};
+
+// ---------------------------------------------------------------------------
+// Adjoint (mp_adjoint): the discrete adjoint of one PLRC step, run backwards.
+
+// One CPML face's adjoint totals, in the layout of CpmlFace: for an E face the
+// adjoint of its psi after the E half plus dt times the adjoint of the E
+// numerator component it feeds; for an H face the adjoint of its psi after the
+// B half plus dt times the adjoint of the B component it feeds.
+template <typename T>
+struct AdjFace {
+  int active, dim, lo, hi, zlo, ex, ey;
+  T *a0, *a1;
+  const T *b, *c;
+};
+
+template <typename T>
+struct AdjParams {
+  int nx, ny, nz;
+  long long plane;
+  double dt;
+  T *Eb[3], *Bb[3];       // adjoint of E and B (full plane layout)
+  T *G[3];                // adjoint of the E numerator of the step (planes 1..nz; 0 elsewhere)
+  T *psib[3][3];          // adjoint of the PLRC accumulators, pairs over planes mz0..mz1
+  const T *En[3];         // E before the step
+  const T *En1[3];        // E after the step
+  const T *ikE[3], *ikH[3], *ikH_bzy;
+  double pD[3][2], pxi[3][2], pC[3][2];  // active poles, FP64
+  double sumChi0, sumXi0, chi, eps, eps_bg;
+  int np, mz0, mz1, nonlin;
+  AdjFace<T> fe[6], fh[6];
+  DesignParams design;
+  double *grad[3];        // dJ/d eps, dJ/d Delta-eps factor, dJ/d chi factor (box-sized, FP64)
+  // objective term of the state before the step (added when add_obj)
+  int obj_kind, add_obj;
+  int ox0, ox1, oy0, oy1, oz0, oz1;  // 0-based x/y, MPulse z
+  double obj_f;           // 2 dt (E^2 box) or dt dx dy (Sz plane)
+  const T *obx, *oby;     // Bx, By of that state on the Sz plane (plane-sized)
 };
 
 // Incident-source plane evaluation.

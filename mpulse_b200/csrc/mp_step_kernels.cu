@@ -40,7 +40,7 @@
 
 namespace mpb {
 
-template <typename T, int MODE, int NP>
+template <typename T, int MODE, int NP, bool DESIGN>
 __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EParams<T> p) {
   typedef typename Vec2<T>::type T2;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based: MPulse i + 1
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
         for (int c = 0; c < 3; ++c) q[n][c] = reinterpret_cast<const T2 *>(p.psi[n][c])[pi];
     }
     T exn, eyn, ezn;
-    e_cell<T, MODE, NP>(p, i, j, k, col, med, v, ikx, iky, ikz, q, exn, eyn, ezn);
+    e_cell<T, MODE, NP, DESIGN>(p, i, j, k, col, med, v, ikx, iky, ikz, q, exn, eyn, ezn);
     // ---- stores
     Ex[base + col] = exn;
     Ey[base + col] = eyn;
@@ -189,26 +189,31 @@ static dim3 grid_for(int nx, int ny, int nk, int kchunk) {
   return dim3((nx + 31) / 32, (ny + 7) / 8, (nk + kchunk - 1) / kchunk);
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, bool DESIGN>
 static cudaError_t launch_e_np(const EParams<T> &p, int np, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
   const dim3 g = grid_for(p.nx, p.ny, nk, p.kchunk), b(32, 8, 1);
   switch (np) {
-    case 0: e_half_kernel<T, MODE, 0><<<g, b, 0, st>>>(p); break;
-    case 1: e_half_kernel<T, MODE, 1><<<g, b, 0, st>>>(p); break;
-    case 2: e_half_kernel<T, MODE, 2><<<g, b, 0, st>>>(p); break;
-    default: e_half_kernel<T, MODE, 3><<<g, b, 0, st>>>(p); break;
+    case 0: e_half_kernel<T, MODE, 0, DESIGN><<<g, b, 0, st>>>(p); break;
+    case 1: e_half_kernel<T, MODE, 1, DESIGN><<<g, b, 0, st>>>(p); break;
+    case 2: e_half_kernel<T, MODE, 2, DESIGN><<<g, b, 0, st>>>(p); break;
+    default: e_half_kernel<T, MODE, 3, DESIGN><<<g, b, 0, st>>>(p); break;
   }
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_e_half(const EParams<T> &p, int mode, int np, cudaStream_t st) {
+  // design regions exist only with the PLRC solvers
+  const bool design = p.design.x0 <= p.design.x1;
   switch (mode) {
-    case MODE_PLAIN: return launch_e_np<T, MODE_PLAIN>(p, 0, st);
-    case MODE_NL: return launch_e_np<T, MODE_NL>(p, 0, st);
-    case MODE_PLRC_LIN: return launch_e_np<T, MODE_PLRC_LIN>(p, np, st);
-    default: return launch_e_np<T, MODE_PLRC_NONLIN>(p, np, st);
+    case MODE_PLAIN: return launch_e_np<T, MODE_PLAIN, false>(p, 0, st);
+    case MODE_NL: return launch_e_np<T, MODE_NL, false>(p, 0, st);
+    case MODE_PLRC_LIN:
+      return design ? launch_e_np<T, MODE_PLRC_LIN, true>(p, np, st) : launch_e_np<T, MODE_PLRC_LIN, false>(p, np, st);
+    default:
+      return design ? launch_e_np<T, MODE_PLRC_NONLIN, true>(p, np, st)
+                    : launch_e_np<T, MODE_PLRC_NONLIN, false>(p, np, st);
   }
 }
 

@@ -25,7 +25,7 @@ EXPORTED = (
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
-    "mp_field_energy_noalloc",
+    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint",
 )
 
 _lib = None
@@ -84,6 +84,10 @@ def lib():
     L.mp_field_energy_noalloc.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double, vp, dp]
     L.mp_field_energy_noalloc.restype = C.c_int
+    L.mp_objective.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp]
+    L.mp_objective.restype = C.c_int
+    L.mp_adjoint.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp, dp, dp, dp]
+    L.mp_adjoint.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
@@ -194,3 +198,31 @@ class Simulation:
     @property
     def launches(self) -> int:
         return lib().mp_launch_count(self._h)
+
+    # -- design region, objective, adjoint
+    def upload_design(self, name: str, arr):
+        """One of abi.DESIGN_NAMES, shaped like abi.design_shape(cfg)."""
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        self._check(lib().mp_upload(self._h, name.encode(), _dptr(a), a.size))
+
+    def download_design(self, name: str) -> np.ndarray:
+        shape = abi.design_shape(self.cfg)
+        out = np.empty(int(np.prod(shape)), dtype=np.float64)
+        self._check(lib().mp_download(self._h, name.encode(), _dptr(out), out.size))
+        return out.reshape(shape)
+
+    def objective(self, adj: abi.AdjointConfig) -> float:
+        """Runs adj.steps steps and returns the objective J (mp_objective)."""
+        J = C.c_double()
+        self._check(lib().mp_objective(self._h, C.byref(adj), C.byref(J)))
+        return J.value
+
+    def adjoint(self, adj: abi.AdjointConfig) -> tuple[float, dict]:
+        """J and its gradient with respect to the design maps (mp_adjoint):
+        {"DesignEps": .., "DesignDepsScale": .., "DesignChiScale": ..}."""
+        shape = abi.design_shape(self.cfg)
+        n = int(np.prod(shape))
+        g = [np.empty(n) for _ in range(3)]
+        J = C.c_double()
+        self._check(lib().mp_adjoint(self._h, C.byref(adj), C.byref(J), _dptr(g[0]), _dptr(g[1]), _dptr(g[2])))
+        return J.value, {name: a.reshape(shape) for name, a in zip(abi.DESIGN_NAMES, g)}

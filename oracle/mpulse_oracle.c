@@ -98,6 +98,10 @@ typedef struct mpo_sim {
   src_state src[MP_MAX_SOURCES];
   double complex dchi0[3], dxi0[3], crec[3];
   double sumChi0, sumXi0;
+  /* design region: per-cell eps_infinity, Delta-eps factor, chi factor */
+  int design;
+  box3 dbox;
+  double *deps, *dscale, *dchi;
   long long time;
   int newton_fail;
   char err[256];
@@ -931,32 +935,46 @@ static void plrc_step_d(mpo_sim *s, int i, int j, int k, double Jx, double Jy, d
   const double kappaEdx = s->kapE[0][i] * c->dx;
   const double kappaEdy = s->kapE[1][j] * c->dy;
   const double kappaEdz = s->kapE[2][k] * c->dz;
+  /* a design cell scales every pole's coefficients by its Delta-eps factor
+   * and has its own eps_infinity and chi factor (all 1 / eps elsewhere, which
+   * leaves the arithmetic of the reference unchanged) */
+  int dcell = 0;
+  double eps_c = c->eps, sc = 1.0, uc = 1.0;
+  if (s->design && i >= s->dbox.lo[0] && i <= s->dbox.hi[0] && j >= s->dbox.lo[1] && j <= s->dbox.hi[1] &&
+      k >= s->dbox.lo[2] && k <= s->dbox.hi[2]) {
+    const size_t di = box_index(&s->dbox, i, j, k);
+    dcell = 1;
+    eps_c = s->deps[di];
+    sc = s->dscale[di];
+    uc = s->dchi[di];
+  }
   double Psix = 0, Psiy = 0, Psiz = 0;
   if (med) {
     for (int n = 0; n < 3; ++n) {
-      const double complex D = s->dchi0[n] - s->dxi0[n];
+      const double complex D = dcell ? sc * (s->dchi0[n] - s->dxi0[n]) : s->dchi0[n] - s->dxi0[n];
+      const double complex Xi = dcell ? sc * s->dxi0[n] : s->dxi0[n];
       double complex px = D * ex + CMPLX(s->psiR[n][0][g], s->psiI[n][0][g]);
       double complex py = D * ey + CMPLX(s->psiR[n][1][g], s->psiI[n][1][g]);
       double complex pz = D * ez + CMPLX(s->psiR[n][2][g], s->psiI[n][2][g]);
       Psix += creal(px);
       Psiy += creal(py);
       Psiz += creal(pz);
-      px = s->dxi0[n] * ex + s->crec[n] * px;
-      py = s->dxi0[n] * ey + s->crec[n] * py;
-      pz = s->dxi0[n] * ez + s->crec[n] * pz;
+      px = Xi * ex + s->crec[n] * px;
+      py = Xi * ey + s->crec[n] * py;
+      pz = Xi * ez + s->crec[n] * pz;
       s->psiR[n][0][g] = creal(px); s->psiI[n][0][g] = cimag(px);
       s->psiR[n][1][g] = creal(py); s->psiI[n][1][g] = cimag(py);
       s->psiR[n][2][g] = creal(pz); s->psiI[n][2][g] = cimag(pz);
     }
   }
-  const double eps = med ? c->eps : c->eps_bg;
-  const double sumChi0 = med ? s->sumChi0 : 0.0, sumXi0 = med ? s->sumXi0 : 0.0;
+  const double eps = med ? eps_c : c->eps_bg;
+  const double sumChi0 = med ? sc * s->sumChi0 : 0.0, sumXi0 = med ? sc * s->sumXi0 : 0.0;
   const double sigma = 0.5 * 0.0 * dt; /* Sigma = 0 each step (fdtd_plrc.t:129) */
   const double cbx = (Bz[g] - Bz[IDX(s, i, j - 1, k)]) / kappaEdy - (By[g] - By[IDX(s, i, j, k - 1)]) / kappaEdz;
   const double cby = (Bx[g] - Bx[IDX(s, i, j, k - 1)]) / kappaEdz - (Bz[g] - Bz[IDX(s, i - 1, j, k)]) / kappaEdx;
   const double cbz = (By[g] - By[IDX(s, i - 1, j, k)]) / kappaEdx - (Bx[g] - Bx[IDX(s, i, j - 1, k)]) / kappaEdy;
   if (c->solver == MP_SOLVER_PLRC_LIN) {
-    const double denom = eps + (sumChi0 - sumXi0) + sigma;
+    const double denom = dcell ? eps + sc * (s->sumChi0 - s->sumXi0) + sigma : eps + (sumChi0 - sumXi0) + sigma;
     const double numer = eps - sumXi0 - sigma;
     Ex[g] = (numer * ex + (dt * (cbx + Jx) + Psix)) / denom;
     Ey[g] = (numer * ey + (dt * (cby + Jy) + Psiy)) / denom;
@@ -964,7 +982,7 @@ static void plrc_step_d(mpo_sim *s, int i, int j, int k, double Jx, double Jy, d
     return;
   }
   /* nonlinear core */
-  const double chi = med ? c->chi : 0.0;
+  const double chi = med ? uc * c->chi : 0.0;
   const double denom = eps + sumChi0 - sumXi0 + sigma;
   const double numer = eps - sumXi0 - sigma;
   double E2 = ex * ex + ey * ey + ez * ez;
@@ -1203,6 +1221,33 @@ int mpo_create(const mp_config *cfg, mpo_sim **out) {
   if (has_mag_currents(s))
     for (int c = 0; c < 3; ++c) s->Mt[c] = calloc(n, sizeof(double));
   if (plrc) plrc_coefficients(s);
+  const int *db = cfg->design_box;
+  if (db[0] <= db[1]) {
+    if (!plrc) {
+      mpo_destroy(s);
+      return fail(g_create_err, "a design region needs a PLRC solver");
+    }
+    if (db[0] < 1 || db[1] > cfg->nx || db[2] < 1 || db[2] > db[3] || db[3] > cfg->ny || db[4] < 1 ||
+        db[4] > db[5] || db[5] > cfg->nz || db[4] < cfg->medium_z0 || db[5] > cfg->medium_z1) {
+      mpo_destroy(s);
+      return fail(g_create_err, "design box outside the interior or the medium");
+    }
+    s->design = 1;
+    for (int d = 0; d < 3; ++d) {
+      s->dbox.lo[d] = db[2 * d];
+      s->dbox.hi[d] = db[2 * d + 1];
+      s->dbox.dims[d] = db[2 * d + 1] - db[2 * d] + 1;
+    }
+    const size_t nd = box_size(&s->dbox);
+    s->deps = malloc(nd * sizeof(double));
+    s->dscale = malloc(nd * sizeof(double));
+    s->dchi = malloc(nd * sizeof(double));
+    for (size_t q = 0; q < nd; ++q) {
+      s->deps[q] = cfg->eps;
+      s->dscale[q] = 1.0;
+      s->dchi[q] = 1.0;
+    }
+  }
   *out = s;
   return MP_OK;
 }
@@ -1217,6 +1262,9 @@ void mpo_destroy(mpo_sim *s) {
   for (int l = 0; l < s->nH; ++l) { free(s->Hlay[l].psi[0]); free(s->Hlay[l].psi[1]); free(s->Hlay[l].b); free(s->Hlay[l].c); }
   for (int q = 0; q < MP_MAX_SOURCES; ++q)
     for (int h = 0; h < 2; ++h) { free(s->src[q].gs[h].F1); free(s->src[q].gs[h].F2); }
+  free(s->deps);
+  free(s->dscale);
+  free(s->dchi);
   free(s);
 }
 
@@ -1240,7 +1288,21 @@ size_t mpo_field_size(const mpo_sim *s) {
 
 /* Plane layout <-> ghost layout.  Upload fills the x/y ghosts with their
  * periodic images (the state after Storage::applyBoundary). */
+static double *design_by_name(mpo_sim *s, const char *name) {
+  if (!s->design) return NULL;
+  if (!strcmp(name, "DesignEps")) return s->deps;
+  if (!strcmp(name, "DesignDepsScale")) return s->dscale;
+  if (!strcmp(name, "DesignChiScale")) return s->dchi;
+  return NULL;
+}
+
 int mpo_upload(mpo_sim *s, const char *name, const double *h, size_t count) {
+  double *d = design_by_name(s, name);
+  if (d) {
+    if (count != box_size(&s->dbox)) return MP_ERR_INVALID;
+    memcpy(d, h, count * sizeof(double));
+    return MP_OK;
+  }
   double *f = field_by_name(s, name);
   if (!f) return MP_ERR_NAME;
   if (count != mpo_field_size(s)) return MP_ERR_INVALID;
@@ -1266,6 +1328,12 @@ int mpo_upload(mpo_sim *s, const char *name, const double *h, size_t count) {
 }
 
 int mpo_download(mpo_sim *s, const char *name, double *h, size_t count) {
+  double *d = design_by_name(s, name);
+  if (d) {
+    if (count != box_size(&s->dbox)) return MP_ERR_INVALID;
+    memcpy(h, d, count * sizeof(double));
+    return MP_OK;
+  }
   double *f = field_by_name(s, name);
   if (!f) return MP_ERR_NAME;
   if (count != mpo_field_size(s)) return MP_ERR_INVALID;
@@ -1323,4 +1391,85 @@ int mpo_source_field(mpo_sim *s, int src, int which, int i, int j, int l, long l
   if (which) src_efield(s, src, i, j, l, time, out);
   else src_hfield(s, src, i, j, l, time, out);
   return MP_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Objectives of mp_objective (additions to MPulse, no reference counterpart):
+ * J = dt sum_n sum_box |E|^2 or dt dx dy sum_n sum_plane (Ex By - Ey Bx),
+ * after each step, accumulated in FP64 in x-fastest order. */
+static double objective_term(const mpo_sim *s, const mp_adjoint_config *a) {
+  const double *Ex = s->F[0], *Ey = s->F[1], *Ez = s->F[2], *Bx = s->F[3], *By = s->F[4];
+  double acc = 0;
+  if (a->kind == MP_OBJ_E2_BOX) {
+    for (int k = a->box[4]; k <= a->box[5]; ++k)
+      for (int j = a->box[2]; j <= a->box[3]; ++j)
+        for (int i = a->box[0]; i <= a->box[1]; ++i) {
+          const size_t g = IDX(s, i, j, k);
+          acc += Ex[g] * Ex[g] + Ey[g] * Ey[g] + Ez[g] * Ez[g];
+        }
+    return s->cfg.dt * acc;
+  }
+  const int k = a->box[4];
+  for (int j = a->box[2]; j <= a->box[3]; ++j)
+    for (int i = a->box[0]; i <= a->box[1]; ++i) {
+      const size_t g = IDX(s, i, j, k);
+      acc += Ex[g] * By[g] - Ey[g] * Bx[g];
+    }
+  return s->cfg.dt * s->cfg.dx * s->cfg.dy * acc;
+}
+
+int mpo_objective(mpo_sim *s, const mp_adjoint_config *a, double *J) {
+  if (a->kind != MP_OBJ_E2_BOX && a->kind != MP_OBJ_SZ_PLANE) return MP_ERR_INVALID;
+  double acc = 0;
+  for (int n = 0; n < a->steps; ++n) {
+    const int rc = mpo_step(s, 1);
+    if (rc != MP_OK) return rc;
+    acc += objective_term(s, a);
+  }
+  *J = acc;
+  return MP_OK;
+}
+
+/* Coefficient access for the test harness's adjoint restatement. */
+int mpo_kappa(const mpo_sim *s, int isH, int dim, double *out, size_t n) {
+  const int nn[3] = {s->cfg.nx, s->cfg.ny, s->cfg.nz};
+  if (dim < 0 || dim > 2 || n != (size_t)nn[dim] + 2) return MP_ERR_INVALID;
+  memcpy(out, isH ? s->kapH[dim] : s->kapE[dim], n * sizeof(double));
+  return MP_OK;
+}
+
+int mpo_cpml_count(const mpo_sim *s, int isH) { return isH ? s->nH : s->nE; }
+
+/* info: dir, dim, lo[3], hi[3]; b and c have hi[dim] - lo[dim] + 1 entries
+ * (c not yet divided by delta).  With another n only info is filled. */
+int mpo_cpml_layer(const mpo_sim *s, int isH, int l, int info[8], double *b, double *c, size_t n, double *delta) {
+  const int cnt = isH ? s->nH : s->nE;
+  if (l < 0 || l >= cnt) return MP_ERR_INVALID;
+  const cpml_layer *L = isH ? &s->Hlay[l] : &s->Elay[l];
+  const size_t len = (size_t)L->box.dims[L->dim];
+  info[0] = L->dir;
+  info[1] = L->dim;
+  for (int d = 0; d < 3; ++d) {
+    info[2 + d] = L->box.lo[d];
+    info[5 + d] = L->box.hi[d];
+  }
+  if (n != len) return MP_ERR_INVALID; /* info is filled; n tells the caller's buffer length */
+  memcpy(b, L->b, len * sizeof(double));
+  memcpy(c, L->c, len * sizeof(double));
+  *delta = L->delta;
+  return MP_OK;
+}
+
+/* dchi0, dxi0, crec (re, im) for the 3 pole slots, then sumChi0, sumXi0. */
+void mpo_plrc_coefficients(const mpo_sim *s, double out[20]) {
+  for (int n = 0; n < 3; ++n) {
+    out[2 * n] = creal(s->dchi0[n]);
+    out[2 * n + 1] = cimag(s->dchi0[n]);
+    out[6 + 2 * n] = creal(s->dxi0[n]);
+    out[6 + 2 * n + 1] = cimag(s->dxi0[n]);
+    out[12 + 2 * n] = creal(s->crec[n]);
+    out[12 + 2 * n + 1] = cimag(s->crec[n]);
+  }
+  out[18] = s->sumChi0;
+  out[19] = s->sumXi0;
 }

@@ -52,6 +52,17 @@ def lib():
         L.mpo_source_field.restype = C.c_int
         L.mpo_field_energy.argtypes = [C.c_void_p]
         L.mpo_field_energy.restype = C.c_double
+        L.mpo_objective.argtypes = [C.c_void_p, C.POINTER(abi.AdjointConfig), C.POINTER(C.c_double)]
+        L.mpo_objective.restype = C.c_int
+        L.mpo_kappa.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_size_t]
+        L.mpo_kappa.restype = C.c_int
+        L.mpo_cpml_count.argtypes = [C.c_void_p, C.c_int]
+        L.mpo_cpml_count.restype = C.c_int
+        L.mpo_cpml_layer.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.c_size_t, C.POINTER(C.c_double)]
+        L.mpo_cpml_layer.restype = C.c_int
+        L.mpo_plrc_coefficients.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.mpo_plrc_coefficients.restype = None
         _lib = L
     return _lib
 
@@ -105,6 +116,47 @@ class OracleSim:
 
     def field_energy(self) -> float:
         return lib().mpo_field_energy(self.h)
+
+    def upload_design(self, name: str, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        rc = lib().mpo_upload(self.h, name.encode(), _dptr(a), a.size)
+        if rc != abi.MP_OK:
+            raise ValueError(f"mpo_upload({name}): {rc}")
+
+    def objective(self, adj: abi.AdjointConfig) -> float:
+        """Runs adj.steps steps and returns J (mp_objective's definition)."""
+        J = C.c_double()
+        rc = lib().mpo_objective(self.h, C.byref(adj), C.byref(J))
+        if rc != abi.MP_OK:
+            raise ValueError(f"mpo_objective: {abi.STATUS_NAMES.get(rc, rc)}")
+        return J.value
+
+    def kappa(self, isH: int, dim: int) -> np.ndarray:
+        n = (self.cfg.nx, self.cfg.ny, self.cfg.nz)[dim] + 2
+        out = np.empty(n)
+        assert lib().mpo_kappa(self.h, isH, dim, _dptr(out), n) == abi.MP_OK
+        return out
+
+    def cpml_layers(self, isH: int):
+        """[(dir, dim, lo[3], hi[3], b, c, delta)] of the CPML currents."""
+        out = []
+        for l in range(lib().mpo_cpml_count(self.h, isH)):
+            info = (C.c_int * 8)()
+            d = C.c_double()
+            dummy = np.empty(1)
+            lib().mpo_cpml_layer(self.h, isH, l, info, _dptr(dummy), _dptr(dummy), 0, C.byref(d))
+            length = info[5 + info[1]] - info[2 + info[1]] + 1
+            b = np.empty(length)
+            c = np.empty(length)
+            assert lib().mpo_cpml_layer(self.h, isH, l, info, _dptr(b), _dptr(c), length, C.byref(d)) == abi.MP_OK
+            out.append((info[0], info[1], tuple(info[2:5]), tuple(info[5:8]), b, c, d.value))
+        return out
+
+    def plrc_coefficients(self) -> dict:
+        o = np.empty(20)
+        lib().mpo_plrc_coefficients(self.h, _dptr(o))
+        z = lambda a: o[a:a + 6:2] + 1j * o[a + 1:a + 6:2]  # noqa: E731
+        return {"dchi0": z(0), "dxi0": z(6), "crec": z(12), "sumChi0": o[18], "sumXi0": o[19]}
 
     def source_field(self, src: int, which: int, i: int, j: int, l: int, time: int):
         out = np.zeros(3)

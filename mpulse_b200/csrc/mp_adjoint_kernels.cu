@@ -20,125 +20,144 @@
 //   adj_b_kernel (B cells, planes 0..nz)  gathers the adjoint of B from G
 //     through the transposed curl_E and the E-face totals, adds the
 //     objective's B term and advances its H-face totals.
-// All arithmetic is FP64; the adjoint state is stored in the precision of the
-// forward state and the gradients in FP64.  Memory-bound, one thread per cell.
+// The Kerr linearisation and the gradient accumulation are FP64; the rest is
+// in the precision of the forward state.  Memory-bound; one thread per (x, y)
+// column and chunk of planes.
 #include "mp_device.h"
 
 #include <cuda_runtime.h>
+
+// Resident blocks per SM asked of the register allocator, per precision.
+#ifndef MPB_ADJ_E_MIN_F
+#define MPB_ADJ_E_MIN_F 2
+#endif
+#ifndef MPB_ADJ_E_MIN_D
+#define MPB_ADJ_E_MIN_D 2
+#endif
+#ifndef MPB_ADJ_B_MIN_F
+#define MPB_ADJ_B_MIN_F 3
+#endif
+#ifndef MPB_ADJ_B_MIN_D
+#define MPB_ADJ_B_MIN_D 2
+#endif
 
 namespace mpb {
 
 namespace {
 
+// Position of axis index idx in a face entry (-1: outside its layers).
 template <typename T>
-__device__ __forceinline__ bool face_at(const AdjFace<T> &F, int i, int j, int k, int nx, int ny, int nz,
-                                        long long &li, int &idx) {
-  if (!F.active) return false;
-  idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
-  if (idx < F.lo || idx > F.hi) return false;
-  if (F.dim == 2) {
-    li = ((long long)(k - F.lo) * ny + j) * nx + i;
-    return true;
-  }
-  if (k < F.zlo || k > nz) return false;  // x / y faces cover planes zlo..nz
-  if (F.dim == 0) li = ((long long)(k - F.zlo) * ny + j) * F.ex + (i + 1 - F.lo);
-  else li = ((long long)(k - F.zlo) * F.ey + (j + 1 - F.lo)) * nx + i;
-  return true;
+__device__ __forceinline__ int face_pos(const AdjFace<T> &F, int idx) {
+  if (!F.active) return -1;
+  if (idx >= F.lo0 && idx <= F.hi0) return idx - F.lo0;
+  if (idx >= F.lo1 && idx <= F.hi1) return F.n0 + idx - F.lo1;
+  return -1;
 }
 
-// c * total of a face at (i, j, k), zero outside the face
-template <typename T>
-__device__ __forceinline__ void face_w(const AdjFace<T> &F, int i, int j, int k, int nx, int ny, int nz, double &w0,
-                                       double &w1) {
-  long long li;
-  int idx;
-  if (face_at(F, i, j, k, nx, ny, nz, li, idx)) {
-    const double c = (double)F.c[idx];
-    w0 = c * (double)F.a0[li];
-    w1 = c * (double)F.a1[li];
+// Element of the x (D = 0) or y (D = 1) entry at plane k, axis position pos,
+// column (i, j).
+template <int D, typename T>
+__device__ __forceinline__ long long face_xy_index(const AdjFace<T> &F, int pos, int i, int j, int k, int nx,
+                                                   int ny) {
+  return D == 0 ? ((long long)(k - F.zlo) * ny + j) * F.ex + pos : ((long long)(k - F.zlo) * F.ey + pos) * nx + i;
+}
+
+// The components fed by psi0 / psi1 of a face along D (cpml_border.cpp:357-386):
+// x faces (y, z), y faces (z, x), z faces (x, y).
+template <int D, typename R>
+__device__ __forceinline__ R comp0(const R v[3]) {
+  return D == 0 ? v[1] : (D == 1 ? v[2] : v[0]);
+}
+template <int D, typename R>
+__device__ __forceinline__ R comp1(const R v[3]) {
+  return D == 0 ? v[2] : (D == 1 ? v[0] : v[1]);
+}
+
+// c * total at element li of an entry, or zero for pos < 0
+template <typename T, typename R>
+__device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, long long li, R c, R &w0, R &w1) {
+  if (pos >= 0) {
+    w0 = c * R(F.a0[li]);
+    w1 = c * R(F.a1[li]);
   } else {
-    w0 = w1 = 0.0;
+    w0 = w1 = R(0);
   }
-}
-
-// components fed by psi0 / psi1 of a face along dim (cpml_border.cpp:357-386)
-__device__ __forceinline__ void face_comps(int dim, int &c0, int &c1) {
-  if (dim == 2) { c0 = 0; c1 = 1; }
-  else if (dim == 0) { c0 = 1; c1 = 2; }
-  else { c0 = 2; c1 = 0; }
 }
 
 }  // namespace
 
+// Arithmetic is in T (the precision of the state); the Kerr linearisation and
+// the design gradients are FP64.  One thread per (x, y) column marches up a
+// chunk of planes, carrying the z-neighbours in registers.
 template <typename T, int NP>
-__global__ void __launch_bounds__(256) adj_e_kernel(const AdjParams<T> p) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_ADJ_E_MIN_D)
+    adj_e_kernel(const AdjParams<T> p) {
+  typedef T R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z + 1;
   if (i >= p.nx || j >= p.ny) return;
-  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int k0 = 1 + blockIdx.z * p.kchunk_e;
+  const int k1 = min(k0 + p.kchunk_e - 1, p.nz);
+  if (k0 > k1) return;
+  const int nx = p.nx, ny = p.ny;
   const int im = i == 0 ? nx - 1 : i - 1;
   const int jm = j == 0 ? ny - 1 : j - 1;
-  const long long pl = p.plane, col = (long long)j * nx + i;
-  const long long c0 = (long long)k * pl + col;
-  const long long cxm = (long long)k * pl + (long long)j * nx + im;
-  const long long cym = (long long)k * pl + (long long)jm * nx + i;
-  const long long czm = c0 - pl;
-  const double dt = p.dt;
-
-  // ---- adjoint of E' (B half transposed)
-  double a[3] = {(double)p.Eb[0][c0], (double)p.Eb[1][c0], (double)p.Eb[2][c0]};
+  const long long pl = p.plane;
+  const int col = j * nx + i, colxm = j * nx + im, colym = jm * nx + i;
+  const R dt = R(p.dt);
+  const R kxi = p.ikH[0][i + 1], kxm = p.ikH[0][im + 1];
+  const R kyj = p.ikH[1][j + 1], kym = p.ikH[1][jm + 1];
+  const R bzj = p.ikH_bzy[j + 1], bzm = p.ikH_bzy[jm + 1];
+  const T *Bx = p.Bb[0], *By = p.Bb[1], *Bz = p.Bb[2];
+  const AdjFace<T> &HX = p.fh[0], &HY = p.fh[1], &HZ = p.fh[2];
+  const AdjFace<T> &EX = p.fe[0], &EY = p.fe[1], &EZ = p.fe[2];
+  // H faces at this column and at x-1 / y-1; E faces at this column
+  const int hxo = face_pos(HX, i + 1), hxm = face_pos(HX, im + 1);
+  const int hyo = face_pos(HY, j + 1), hym = face_pos(HY, jm + 1);
+  const R hxco = hxo >= 0 ? R(HX.c[i + 1]) : R(0), hxcm = hxm >= 0 ? R(HX.c[im + 1]) : R(0);
+  const R hyco = hyo >= 0 ? R(HY.c[j + 1]) : R(0), hycm = hym >= 0 ? R(HY.c[jm + 1]) : R(0);
+  const int exo = face_pos(EX, i + 1), eyo = face_pos(EY, j + 1);
+  const R exb = exo >= 0 ? R(EX.b[i + 1]) : R(0), eyb = eyo >= 0 ? R(EY.b[j + 1]) : R(0);
+  // the z H face's c * total at plane k - 1, carried
+  R cw0, cw1;
   {
-    const double kxi = p.ikH[0][i + 1], kxm = p.ikH[0][im + 1];
-    const double kyj = p.ikH[1][j + 1], kym = p.ikH[1][jm + 1];
-    const double kzk = p.ikH[2][k], kzm = p.ikH[2][k - 1];
-    const double bzj = p.ikH_bzy[j + 1], bzm = p.ikH_bzy[jm + 1];
-    const T *Bx = p.Bb[0], *By = p.Bb[1], *Bz = p.Bb[2];
-    // Bx' = .. + dt ((ey(k+1) - ey) ikz - (ez(j+1) - ez) iky)
-    a[1] += dt * (kzm * (double)Bx[czm] - kzk * (double)Bx[c0]);
-    a[2] += dt * (-kym * (double)Bx[cym] + kyj * (double)Bx[c0]);
-    // By' = .. + dt ((ez(i+1) - ez) ikx - (ex(k+1) - ex) ikz)
-    a[2] += dt * (kxm * (double)By[cxm] - kxi * (double)By[c0]);
-    a[0] += dt * (-kzm * (double)By[czm] + kzk * (double)By[c0]);
-    // Bz' = .. + dt ((ex(j+1) - ex) iky_bz - (ey(i+1) - ey) ikx)
-    a[0] += dt * (bzm * (double)Bz[cym] - bzj * (double)Bz[c0]);
-    a[1] += dt * (-kxm * (double)Bz[cxm] + kxi * (double)Bz[c0]);
+    const int pz = face_pos(HZ, k0 - 1);
+    face_w(HZ, pz, (long long)pz * pl + col, pz >= 0 ? R(HZ.c[k0 - 1]) : R(0), cw0, cw1);
   }
-#pragma unroll
-  for (int f = 0; f < 6; ++f) {
-    const AdjFace<T> &F = p.fh[f];
-    if (!F.active) continue;
-    double w0o, w1o, w0m, w1m;
-    face_w(F, i, j, k, nx, ny, nz, w0o, w1o);
-    if (F.dim == 2) {
-      face_w(F, i, j, k - 1, nx, ny, nz, w0m, w1m);
-      a[1] += w0m - w0o;
-      a[0] += w1o - w1m;
-    } else if (F.dim == 0) {
-      face_w(F, im, j, k, nx, ny, nz, w0m, w1m);
-      a[2] += w0m - w0o;
-      a[1] += w1o - w1m;
-    } else {
-      face_w(F, i, jm, k, nx, ny, nz, w0m, w1m);
-      a[0] += w0m - w0o;
-      a[2] += w1o - w1m;
-    }
-  }
+  const DesignParams &d = p.design;
+  const bool dxy = i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1;
+  const bool oxy = i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
+  R bx_km = Bx[(long long)(k0 - 1) * pl + col];
+  R by_km = By[(long long)(k0 - 1) * pl + col];
 
-  // ---- E half, locally
-  const double En[3] = {(double)p.En[0][c0], (double)p.En[1][c0], (double)p.En[2][c0]};
-  double g[3], ne[3];
-  const bool med = k >= p.mz0 && k <= p.mz1;
-  if (!med) {
-    // background: E' = (eps_bg E + dt (curl + J)) / eps_bg
+  const bool plrc_nl = p.nonlin != 0;
+  for (int k = k0; k <= k1; ++k) {
+    const long long base = (long long)k * pl;
+    const long long c0 = base + col;
+    const bool med = k >= p.mz0 && k <= p.mz1;
+    const bool dcell = med && dxy && k >= d.z0 && k <= d.z1;
+    // ---- every load of this plane first, so that their latencies overlap
+    const R bx = Bx[c0], by = By[c0], bz = Bz[c0];
+    const R bx_ym = Bx[base + colym], by_xm = By[base + colxm], bz_ym = Bz[base + colym], bz_xm = Bz[base + colxm];
+    const R kzk = p.ikH[2][k], kzm = p.ikH[2][k - 1];
+    R a[3] = {R(p.Eb[0][c0]), R(p.Eb[1][c0]), R(p.Eb[2][c0])};
+    const R En[3] = {R(p.En[0][c0]), R(p.En[1][c0]), R(p.En[2][c0])};
+    R En1[3] = {R(0), R(0), R(0)};
+    if (med && (plrc_nl || dcell)) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      g[c] = a[c] / p.eps_bg;
-      ne[c] = p.eps_bg * g[c];
+      for (int c = 0; c < 3; ++c) En1[c] = R(p.En1[c][c0]);
     }
-  } else {
-    const DesignParams &d = p.design;
-    const bool dcell = i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1 && k >= d.z0 && k <= d.z1;
+    const long long pi = ((long long)(k - p.mz0) * ny + j) * nx + i;
+    R pq[NP > 0 ? NP : 1][3][2];
+    if (med) {
+#pragma unroll
+      for (int n = 0; n < NP; ++n)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          pq[n][c][0] = p.psib[n][c][2 * pi];
+          pq[n][c][1] = p.psib[n][c][2 * pi + 1];
+        }
+    }
     long long di = 0;
     double e = p.eps, s = 1.0, u = 1.0;
     if (dcell) {
@@ -147,186 +166,304 @@ __global__ void __launch_bounds__(256) adj_e_kernel(const AdjParams<T> p) {
       s = d.dscale[di];
       u = d.chiscale[di];
     }
-    const double dD = p.sumChi0 - p.sumXi0;
-    const double numer = e - s * p.sumXi0;
-    const double denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
-    const double chi = p.nonlin ? u * p.chi : 0.0;
-    const double A = chi / denom;
-    const double En1[3] = {(double)p.En1[0][c0], (double)p.En1[1][c0], (double)p.En1[2][c0]};
-    double cbar[3], cvec[3], Abar = 0.0;
-    if (p.nonlin) {
-      // E' = r c/|c| with r + A r^3 = |c|: dE'/dc = (I - e e^T) / (1 + A r^2)
-      // + e e^T / (1 + 3 A r^2), dr/dA = -r^3 / (1 + 3 A r^2), c = E' (1 + A r^2)
-      const double r2 = En1[0] * En1[0] + En1[1] * En1[1] + En1[2] * En1[2];
-      const double r = sqrt(r2);
-      const double al = 1.0 / (1.0 + A * r2), be = 1.0 / (1.0 + 3.0 * A * r2);
-      double eh[3] = {0.0, 0.0, 0.0};
-      if (r > 0) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) eh[c] = En1[c] / r;
-      }
-      const double ea = eh[0] * a[0] + eh[1] * a[1] + eh[2] * a[2];
+    // H-face totals (x, y at this column and x-1 / y-1; z at this plane) and
+    // E-face totals of this cell
+    R hx0o, hx1o, hx0m, hx1m, hy0o, hy1o, hy0m, hy1m, hz0, hz1;
+    const long long lhxo = face_xy_index<0>(HX, hxo, i, j, k, nx, ny), lhxm = face_xy_index<0>(HX, hxm, im, j, k, nx, ny);
+    const long long lhyo = face_xy_index<1>(HY, hyo, i, j, k, nx, ny), lhym = face_xy_index<1>(HY, hym, i, jm, k, nx, ny);
+    face_w(HX, hxo, lhxo, hxco, hx0o, hx1o);
+    face_w(HX, hxm, lhxm, hxcm, hx0m, hx1m);
+    face_w(HY, hyo, lhyo, hyco, hy0o, hy1o);
+    face_w(HY, hym, lhym, hycm, hy0m, hy1m);
+    const int hzp = face_pos(HZ, k);
+    face_w(HZ, hzp, (long long)hzp * pl + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1);
+    const long long lexo = face_xy_index<0>(EX, exo, i, j, k, nx, ny), leyo = face_xy_index<1>(EY, eyo, i, j, k, nx, ny);
+    const int ezp = face_pos(EZ, k);
+    const long long lezo = (long long)ezp * pl + col;
+    R ex0 = R(0), ex1 = R(0), ey0 = R(0), ey1 = R(0), ez0 = R(0), ez1 = R(0), ezb = R(0);
+    if (exo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
+    if (eyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
+    if (ezp >= 0) { ez0 = EZ.a0[lezo]; ez1 = EZ.a1[lezo]; ezb = EZ.b[k]; }
+    R obx = R(0), oby = R(0);
+    if (p.add_obj && oxy && p.obj_kind == 2 && k == p.oz0) {
+      obx = p.obx[col];
+      oby = p.oby[col];
+    }
+
+    // ---- adjoint of E' (B half transposed)
+    // Bx' = .. + dt ((ey(k+1) - ey) ikz - (ez(j+1) - ez) iky)
+    a[1] += dt * (kzm * bx_km - kzk * bx);
+    a[2] += dt * (-kym * bx_ym + kyj * bx);
+    // By' = .. + dt ((ez(i+1) - ez) ikx - (ex(k+1) - ex) ikz)
+    a[2] += dt * (kxm * by_xm - kxi * by);
+    a[0] += dt * (-kzm * by_km + kzk * by);
+    // Bz' = .. + dt ((ex(j+1) - ex) iky_bz - (ey(i+1) - ey) ikx)
+    a[0] += dt * (bzm * bz_ym - bzj * bz);
+    a[1] += dt * (-kxm * bz_xm + kxi * bz);
+    // H faces: psi0 / psi1 feed (y, z) on x faces, (z, x) on y faces, (x, y) on
+    // z faces; their differences of E run forward along the axis
+    a[2] += hx0m - hx0o;
+    a[1] += hx1o - hx1m;
+    a[0] += hy0m - hy0o;
+    a[2] += hy1o - hy1m;
+    a[1] += cw0 - hz0;
+    a[0] += hz1 - cw1;
+    cw0 = hz0;
+    cw1 = hz1;
+
+    // ---- E half, locally
+    R g[3], ne[3];
+    if (!med) {
+      // background: E' = (eps_bg E + dt (curl + J)) / eps_bg
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        cbar[c] = al * (a[c] - eh[c] * ea) + be * eh[c] * ea;
-        cvec[c] = En1[c] * (1.0 + A * r2);
+        g[c] = a[c] * R(p.inv_eps_bg);
+        ne[c] = R(p.eps_bg) * g[c];
       }
-      Abar = -ea * r * r2 * be;
     } else {
+      const double dD = p.sumChi0 - p.sumXi0;
+      double denom = 0.0, A = p.A0;
+      R idn = R(p.inv_denom0), numer = R(p.numer0), Rchi = R(p.nonlin ? p.chi : 0.0);
+      if (dcell) {
+        denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
+        A = p.nonlin ? u * p.chi / denom : 0.0;
+        idn = R(1.0 / denom);
+        numer = R(e - s * p.sumXi0);
+        Rchi = R(p.nonlin ? u * p.chi : 0.0);
+      }
+      R cb[3] = {a[0], a[1], a[2]};
+      double Abar = 0.0;
+      if (plrc_nl) {
+        // E' = r c/|c| with r + A r^3 = |c|: dE'/dc = (I - e e^T) / (1 + A r^2)
+        // + e e^T / (1 + 3 A r^2), dr/dA = -r^3 / (1 + 3 A r^2), c = E' (1 + A r^2)
+        const double r2 = (double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2];
+        const double r = sqrt(r2);
+        const double al = 1.0 / (1.0 + A * r2), be = 1.0 / (1.0 + 3.0 * A * r2);
+        const double ir = r > 0 ? 1.0 / r : 0.0;
+        double eh[3], ea = 0.0;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        cbar[c] = a[c];
-        cvec[c] = En1[c];
+        for (int c = 0; c < 3; ++c) {
+          eh[c] = En1[c] * ir;
+          ea += eh[c] * a[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) cb[c] = R(al * (a[c] - eh[c] * ea) + be * eh[c] * ea);
+        Abar = -ea * r * r2 * be;
+      }
+      const R E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[c] = cb[c] * idn;
+      const R Eg = En[0] * g[0] + En[1] * g[1] + En[2] * g[2];
+      const R f = numer + Rchi * E2;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ne[c] = f * g[c] + R(2) * Rchi * En[c] * Eg;
+      // reverse PLRC recursion: psi~bar = conj(Crec) psibar + g
+      double gs = 0.0;
+      const R Rs = R(s);
+#pragma unroll
+      for (int n = 0; n < NP; ++n) {
+        const R Dr = R(p.pD[n][0]), Di = R(p.pD[n][1]);
+        const R Xr = R(p.pxi[n][0]), Xi = R(p.pxi[n][1]);
+        const R Cr = R(p.pC[n][0]), Ci = R(p.pC[n][1]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const R pr = pq[n][c][0], pim = pq[n][c][1];
+          const R tr = Cr * pr + Ci * pim + g[c];
+          const R ti = Cr * pim - Ci * pr;
+          ne[c] += Rs * (Dr * tr + Di * ti + Xr * pr + Xi * pim);
+          if (dcell) {
+            const double CDr = p.pC[n][0] * p.pD[n][0] - p.pC[n][1] * p.pD[n][1];
+            const double CDi = p.pC[n][0] * p.pD[n][1] + p.pC[n][1] * p.pD[n][0];
+            gs += ((double)pr * (p.pxi[n][0] + CDr) + (double)pim * (p.pxi[n][1] + CDi)) * (double)En[c];
+          }
+          pq[n][c][0] = tr;
+          pq[n][c][1] = ti;
+        }
+      }
+      if (dcell) {
+        double SD = 0.0;
+#pragma unroll
+        for (int n = 0; n < NP; ++n) SD += p.pD[n][0];
+        double ge = -Abar * A / denom, gu = 0.0;
+        gs -= Abar * A * dD / denom;
+        // c = E' (1 + A |E'|^2); A = 0 in the linear case
+        const double grow = 1.0 + A * ((double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double cv = (double)En1[c] * grow;
+          ge += (double)g[c] * ((double)En[c] - cv);
+          gs += (double)g[c] * ((SD - p.sumXi0) * (double)En[c] - cv * dD);
+        }
+        if (p.nonlin) {
+          gu = Abar * p.chi / denom;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) gu += (double)g[c] * p.chi * (double)E2 * (double)En[c];
+        }
+        p.grad[0][di] += ge;
+        p.grad[1][di] += gs;
+        p.grad[2][di] += gu;
       }
     }
-    const double E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
+    // the objective's E term of the state before the step
+    if (p.add_obj && oxy) {
+      if (p.obj_kind == 1) {
+        if (k >= p.oz0 && k <= p.oz1) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) g[c] = cbar[c] / denom;
-    const double Eg = En[0] * g[0] + En[1] * g[1] + En[2] * g[2];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) ne[c] = (numer + chi * E2) * g[c] + 2.0 * chi * En[c] * Eg;
-    // reverse PLRC recursion (pairs over the medium planes)
-    double gs = 0.0, SD = 0.0;
-    const long long pi = ((long long)(k - p.mz0) * ny + j) * nx + i;
-#pragma unroll
-    for (int n = 0; n < NP; ++n) {
-      const double Dr = p.pD[n][0], Di = p.pD[n][1];
-      const double Xr = p.pxi[n][0], Xi = p.pxi[n][1];
-      const double Cr = p.pC[n][0], Ci = p.pC[n][1];
-      const double CDr = Cr * Dr - Ci * Di, CDi = Cr * Di + Ci * Dr;
-      SD += Dr;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        T *q = p.psib[n][c] + 2 * pi;
-        const double pr = (double)q[0], pim = (double)q[1];
-        // psi~bar = conj(Crec) psibar + g
-        const double tr = Cr * pr + Ci * pim + g[c];
-        const double ti = Cr * pim - Ci * pr;
-        ne[c] += s * (Dr * tr + Di * ti) + s * (Xr * pr + Xi * pim);
-        gs += pr * (Xr + CDr) * En[c] + pim * (Xi + CDi) * En[c];
-        q[0] = T(tr);
-        q[1] = T(ti);
+          for (int c = 0; c < 3; ++c) ne[c] += R(p.obj_f) * En[c];
+        }
+      } else if (k == p.oz0) {
+        ne[0] += R(p.obj_f) * oby;
+        ne[1] -= R(p.obj_f) * obx;
       }
     }
-    if (dcell) {
-      double ge = -Abar * A / denom, gu = 0.0;
-      gs -= Abar * A * dD / denom;
+
+    // ---- stores
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ge += g[c] * (En[c] - cvec[c]);
-        gs += g[c] * ((SD - p.sumXi0) * En[c] - cvec[c] * dD);
-      }
-      if (p.nonlin) {
-        gu = Abar * p.chi / denom;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) gu += g[c] * p.chi * E2 * En[c];
-      }
-      p.grad[0][di] += ge;
-      p.grad[1][di] += gs;
-      p.grad[2][di] += gu;
+    for (int c = 0; c < 3; ++c) {
+      p.G[c][c0] = T(g[c]);
+      p.Eb[c][c0] = T(ne[c]);
     }
-  }
+    if (med) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) p.G[c][c0] = T(g[c]);
-  // ---- the objective's E term of the state before the step
-  if (p.add_obj) {
-    if (p.obj_kind == 1) {
-      if (i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1 && k >= p.oz0 && k <= p.oz1) {
+      for (int n = 0; n < NP; ++n)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ne[c] += p.obj_f * En[c];
-      }
-    } else if (k == p.oz0 && i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1) {
-      ne[0] += p.obj_f * (double)p.oby[col];
-      ne[1] -= p.obj_f * (double)p.obx[col];
+        for (int c = 0; c < 3; ++c) {
+          p.psib[n][c][2 * pi] = T(pq[n][c][0]);
+          p.psib[n][c][2 * pi + 1] = T(pq[n][c][1]);
+        }
     }
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) p.Eb[c][c0] = T(ne[c]);
-  // ---- E-face totals of this cell: b * total + dt * G
-#pragma unroll
-  for (int f = 0; f < 6; ++f) {
-    const AdjFace<T> &F = p.fe[f];
-    long long li;
-    int idx;
-    if (!face_at(F, i, j, k, nx, ny, nz, li, idx)) continue;
-    int q0, q1;
-    face_comps(F.dim, q0, q1);
-    const double b = (double)F.b[idx];
-    F.a0[li] = T(b * (double)F.a0[li] + dt * g[q0]);
-    F.a1[li] = T(b * (double)F.a1[li] + dt * g[q1]);
+    // E-face totals of this cell: b * total + dt * G
+    if (exo >= 0) {
+      EX.a0[lexo] = T(exb * ex0 + dt * comp0<0>(g));
+      EX.a1[lexo] = T(exb * ex1 + dt * comp1<0>(g));
+    }
+    if (eyo >= 0) {
+      EY.a0[leyo] = T(eyb * ey0 + dt * comp0<1>(g));
+      EY.a1[leyo] = T(eyb * ey1 + dt * comp1<1>(g));
+    }
+    if (ezp >= 0) {
+      EZ.a0[lezo] = T(ezb * ez0 + dt * comp0<2>(g));
+      EZ.a1[lezo] = T(ezb * ez1 + dt * comp1<2>(g));
+    }
+    bx_km = bx;
+    by_km = by;
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) adj_b_kernel(const AdjParams<T> p) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D)
+    adj_b_kernel(const AdjParams<T> p) {
+  typedef T R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;  // 0..nz
   if (i >= p.nx || j >= p.ny) return;
-  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int k0 = blockIdx.z * p.kchunk_b;
+  const int k1 = min(k0 + p.kchunk_b - 1, p.nz);
+  if (k0 > k1) return;
+  const int nx = p.nx, ny = p.ny;
   const int ip = i == nx - 1 ? 0 : i + 1;
   const int jp = j == ny - 1 ? 0 : j + 1;
-  const long long pl = p.plane, col = (long long)j * nx + i;
-  const long long c0 = (long long)k * pl + col;
-  const long long cxp = (long long)k * pl + (long long)j * nx + ip;
-  const long long cyp = (long long)k * pl + (long long)jp * nx + i;
-  const long long czp = c0 + pl;
-  const double dt = p.dt;
-  double b[3] = {(double)p.Bb[0][c0], (double)p.Bb[1][c0], (double)p.Bb[2][c0]};
+  const long long pl = p.plane;
+  const int col = j * nx + i, colxp = j * nx + ip, colyp = jp * nx + i;
+  const R dt = R(p.dt);
+  const R kxi = p.ikE[0][i + 1], kxp = p.ikE[0][ip + 1];
+  const R kyj = p.ikE[1][j + 1], kyp = p.ikE[1][jp + 1];
+  const T *gx = p.G[0], *gy = p.G[1], *gz = p.G[2];
+  const AdjFace<T> &HX = p.fh[0], &HY = p.fh[1], &HZ = p.fh[2];
+  const AdjFace<T> &EX = p.fe[0], &EY = p.fe[1], &EZ = p.fe[2];
+  // E faces at this column and at x+1 / y+1; H faces at this column
+  const int exo = face_pos(EX, i + 1), exp_ = face_pos(EX, ip + 1);
+  const int eyo = face_pos(EY, j + 1), eyp = face_pos(EY, jp + 1);
+  const R exco = exo >= 0 ? R(EX.c[i + 1]) : R(0), excp = exp_ >= 0 ? R(EX.c[ip + 1]) : R(0);
+  const R eyco = eyo >= 0 ? R(EY.c[j + 1]) : R(0), eycp = eyp >= 0 ? R(EY.c[jp + 1]) : R(0);
+  const int hxo = face_pos(HX, i + 1), hyo = face_pos(HY, j + 1);
+  const R hxb = hxo >= 0 ? R(HX.b[i + 1]) : R(0), hyb = hyo >= 0 ? R(HY.b[j + 1]) : R(0);
+  const bool oxy = p.add_obj && p.obj_kind == 2 && i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
+  // G and the z E face's c * total at plane k, carried from the previous plane's k + 1
+  R gx_k = gx[(long long)k0 * pl + col], gy_k = gy[(long long)k0 * pl + col];
+  R zw0, zw1;
   {
-    const T *gx = p.G[0], *gy = p.G[1], *gz = p.G[2];
-    const double kxi = p.ikE[0][i + 1], kxp = p.ikE[0][ip + 1];
-    const double kyj = p.ikE[1][j + 1], kyp = p.ikE[1][jp + 1];
-    const double kzk = p.ikE[2][k], kzp = p.ikE[2][k + 1];
-    // cbx = (bz - bz(j-1)) iky - (by - by(k-1)) ikz
-    b[2] += dt * (kyj * (double)gx[c0] - kyp * (double)gx[cyp]);
-    b[1] += dt * (-kzk * (double)gx[c0] + kzp * (double)gx[czp]);
-    // cby = (bx - bx(k-1)) ikz - (bz - bz(i-1)) ikx
-    b[0] += dt * (kzk * (double)gy[c0] - kzp * (double)gy[czp]);
-    b[2] += dt * (-kxi * (double)gy[c0] + kxp * (double)gy[cxp]);
-    // cbz = (by - by(i-1)) ikx - (bx - bx(j-1)) iky
-    b[1] += dt * (kxi * (double)gz[c0] - kxp * (double)gz[cxp]);
-    b[0] += dt * (-kyj * (double)gz[c0] + kyp * (double)gz[cyp]);
+    const int pz = face_pos(EZ, k0);
+    face_w(EZ, pz, (long long)pz * pl + col, pz >= 0 ? R(EZ.c[k0]) : R(0), zw0, zw1);
   }
-#pragma unroll
-  for (int f = 0; f < 6; ++f) {
-    const AdjFace<T> &F = p.fe[f];
-    if (!F.active) continue;
-    double w0o, w1o, w0p, w1p;
-    face_w(F, i, j, k, nx, ny, nz, w0o, w1o);
-    if (F.dim == 2) {
-      face_w(F, i, j, k + 1, nx, ny, nz, w0p, w1p);
-      b[1] += -w0o + w0p;
-      b[0] += w1o - w1p;
-    } else if (F.dim == 0) {
-      face_w(F, ip, j, k, nx, ny, nz, w0p, w1p);
-      b[2] += -w0o + w0p;
-      b[1] += w1o - w1p;
-    } else {
-      face_w(F, i, jp, k, nx, ny, nz, w0p, w1p);
-      b[0] += -w0o + w0p;
-      b[2] += w1o - w1p;
+
+  for (int k = k0; k <= k1; ++k) {
+    const long long base = (long long)k * pl;
+    const long long c0 = base + col;
+    // ---- every load of this plane first
+    const R gx_kp = gx[c0 + pl], gy_kp = gy[c0 + pl];
+    const R gzk = gz[c0];
+    const R gx_yp = gx[base + colyp], gy_xp = gy[base + colxp], gz_xp = gz[base + colxp], gz_yp = gz[base + colyp];
+    const R kzk = p.ikE[2][k], kzp = p.ikE[2][k + 1];
+    R b[3] = {R(p.Bb[0][c0]), R(p.Bb[1][c0]), R(p.Bb[2][c0])};
+    // E faces: x / y hold planes 1..nz; z at plane k + 1 (plane k carried)
+    const bool ek = k >= 1;
+    R ex0o, ex1o, ex0p, ex1p, ey0o, ey1o, ey0p, ey1p, ez0p, ez1p;
+    face_w(EX, ek ? exo : -1, face_xy_index<0>(EX, exo, i, j, k, nx, ny), exco, ex0o, ex1o);
+    face_w(EX, ek ? exp_ : -1, face_xy_index<0>(EX, exp_, ip, j, k, nx, ny), excp, ex0p, ex1p);
+    face_w(EY, ek ? eyo : -1, face_xy_index<1>(EY, eyo, i, j, k, nx, ny), eyco, ey0o, ey1o);
+    face_w(EY, ek ? eyp : -1, face_xy_index<1>(EY, eyp, i, jp, k, nx, ny), eycp, ey0p, ey1p);
+    const int ezq = face_pos(EZ, k + 1);
+    face_w(EZ, ezq, (long long)ezq * pl + col, ezq >= 0 ? R(EZ.c[k + 1]) : R(0), ez0p, ez1p);
+    // H-face totals of this cell
+    const bool hxk = hxo >= 0 && k >= HX.zlo, hyk = hyo >= 0 && k >= HY.zlo;
+    const long long lhx = face_xy_index<0>(HX, hxo, i, j, k, nx, ny), lhy = face_xy_index<1>(HY, hyo, i, j, k, nx, ny);
+    const int hzp = face_pos(HZ, k);
+    const long long lhz = (long long)hzp * pl + col;
+    R hx0 = R(0), hx1 = R(0), hy0 = R(0), hy1 = R(0), hz0 = R(0), hz1 = R(0), hzb = R(0);
+    if (hxk) { hx0 = HX.a0[lhx]; hx1 = HX.a1[lhx]; }
+    if (hyk) { hy0 = HY.a0[lhy]; hy1 = HY.a1[lhy]; }
+    if (hzp >= 0) { hz0 = HZ.a0[lhz]; hz1 = HZ.a1[lhz]; hzb = HZ.b[k]; }
+    const bool obj = oxy && k == p.oz0;
+    R oex = R(0), oey = R(0);
+    if (obj) {
+      oex = p.En[0][c0];
+      oey = p.En[1][c0];
     }
-  }
-  // the objective's B term of the state before the step (Sz plane)
-  if (p.add_obj && p.obj_kind == 2 && k == p.oz0 && i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1) {
-    b[0] -= p.obj_f * (double)p.En[1][c0];
-    b[1] += p.obj_f * (double)p.En[0][c0];
-  }
+
+    // ---- transposed curl_E and E faces
+    // cbx = (bz - bz(j-1)) iky - (by - by(k-1)) ikz
+    b[2] += dt * (kyj * gx_k - kyp * gx_yp);
+    b[1] += dt * (-kzk * gx_k + kzp * gx_kp);
+    // cby = (bx - bx(k-1)) ikz - (bz - bz(i-1)) ikx
+    b[0] += dt * (kzk * gy_k - kzp * gy_kp);
+    b[2] += dt * (-kxi * gy_k + kxp * gy_xp);
+    // cbz = (by - by(i-1)) ikx - (bx - bx(j-1)) iky
+    b[1] += dt * (kxi * gzk - kxp * gz_xp);
+    b[0] += dt * (-kyj * gzk + kyp * gz_yp);
+    // E faces: psi0 / psi1 feed (y, z) on x faces, (z, x) on y faces, (x, y) on
+    // z faces; their differences of B run backward along the axis
+    b[2] += -ex0o + ex0p;
+    b[1] += ex1o - ex1p;
+    b[0] += -ey0o + ey0p;
+    b[2] += ey1o - ey1p;
+    b[1] += -zw0 + ez0p;
+    b[0] += zw1 - ez1p;
+    zw0 = ez0p;
+    zw1 = ez1p;
+    // the objective's B term of the state before the step (Sz plane)
+    if (obj) {
+      b[0] -= R(p.obj_f) * oey;
+      b[1] += R(p.obj_f) * oex;
+    }
+
+    // ---- stores: B adjoint, H-face totals for the step before (b * total + dt * B adjoint)
 #pragma unroll
-  for (int c = 0; c < 3; ++c) p.Bb[c][c0] = T(b[c]);
-  // H-face totals for the step before: b * total + dt * adjoint of B
-#pragma unroll
-  for (int f = 0; f < 6; ++f) {
-    const AdjFace<T> &F = p.fh[f];
-    long long li;
-    int idx;
-    if (!face_at(F, i, j, k, nx, ny, nz, li, idx)) continue;
-    int q0, q1;
-    face_comps(F.dim, q0, q1);
-    const double bb = (double)F.b[idx];
-    F.a0[li] = T(bb * (double)F.a0[li] + dt * b[q0]);
-    F.a1[li] = T(bb * (double)F.a1[li] + dt * b[q1]);
+    for (int c = 0; c < 3; ++c) p.Bb[c][c0] = T(b[c]);
+    if (hxk) {
+      HX.a0[lhx] = T(hxb * hx0 + dt * comp0<0>(b));
+      HX.a1[lhx] = T(hxb * hx1 + dt * comp1<0>(b));
+    }
+    if (hyk) {
+      HY.a0[lhy] = T(hyb * hy0 + dt * comp0<1>(b));
+      HY.a1[lhy] = T(hyb * hy1 + dt * comp1<1>(b));
+    }
+    if (hzp >= 0) {
+      HZ.a0[lhz] = T(hzb * hz0 + dt * comp0<2>(b));
+      HZ.a1[lhz] = T(hzb * hz1 + dt * comp1<2>(b));
+    }
+    gx_k = gx_kp;
+    gy_k = gy_kp;
   }
 }
 
@@ -355,15 +492,22 @@ __global__ void __launch_bounds__(256) adj_init_kernel(const AdjParams<T> p) {
     p.Eb[c][c0] = T(e[c]);
     p.Bb[c][c0] = T(b[c]);
   }
-  for (int f = 0; f < 6; ++f) {
-    const AdjFace<T> &F = p.fh[f];
-    long long li;
-    int idx;
-    if (!face_at(F, i, j, k, p.nx, p.ny, p.nz, li, idx)) continue;
-    int q0, q1;
-    face_comps(F.dim, q0, q1);
-    F.a0[li] = T(p.dt * b[q0]);
-    F.a1[li] = T(p.dt * b[q1]);
+  // H-face totals: dt times the adjoint of B
+  const int hxo = face_pos(p.fh[0], i + 1), hyo = face_pos(p.fh[1], j + 1), hzo = face_pos(p.fh[2], k);
+  if (hxo >= 0 && k >= p.fh[0].zlo) {
+    const long long li = face_xy_index<0>(p.fh[0], hxo, i, j, k, p.nx, p.ny);
+    p.fh[0].a0[li] = T(p.dt * comp0<0>(b));
+    p.fh[0].a1[li] = T(p.dt * comp1<0>(b));
+  }
+  if (hyo >= 0 && k >= p.fh[1].zlo) {
+    const long long li = face_xy_index<1>(p.fh[1], hyo, i, j, k, p.nx, p.ny);
+    p.fh[1].a0[li] = T(p.dt * comp0<1>(b));
+    p.fh[1].a1[li] = T(p.dt * comp1<1>(b));
+  }
+  if (hzo >= 0) {
+    const long long li = (long long)hzo * p.plane + col;
+    p.fh[2].a0[li] = T(p.dt * comp0<2>(b));
+    p.fh[2].a1[li] = T(p.dt * comp1<2>(b));
   }
 }
 
@@ -417,7 +561,7 @@ __global__ void __launch_bounds__(256) sum_terms_kernel(const double *terms, lon
 
 template <typename T>
 cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
-  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, p.nz);
+  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, (p.nz + p.kchunk_e - 1) / p.kchunk_e);
   switch (p.np) {
     case 0: adj_e_kernel<T, 0><<<g, b, 0, st>>>(p); break;
     case 1: adj_e_kernel<T, 1><<<g, b, 0, st>>>(p); break;
@@ -429,7 +573,7 @@ cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
 
 template <typename T>
 cudaError_t launch_adj_b(const AdjParams<T> &p, cudaStream_t st) {
-  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, p.nz + 1);
+  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b);
   adj_b_kernel<T><<<g, b, 0, st>>>(p);
   return cudaGetLastError();
 }

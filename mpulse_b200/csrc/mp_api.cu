@@ -21,6 +21,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -784,12 +785,19 @@ struct StepTimer {
   bool on = false;
 };
 
+// Per-step callbacks of step_impl: `before(n)` runs before the launches of the
+// n-th step of the call, `after(n)` after them (both may launch work on the
+// stream and return an mp_status).
+struct StepHooks {
+  std::function<int(long long)> before, after;
+};
+
 // Per step: E half, B half.  The injection planes of a block of up to
 // src_batch steps are computed ahead in one launch (they depend on
 // Process::time only), and each half step reads its step's plane pair.
 template <typename T>
 int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer *tm = nullptr,
-              double *acc = nullptr) {
+              double *acc = nullptr, const StepHooks *hooks = nullptr) {
   const size_t pl = size_t(c->plane);
   int t = 0;
   while (t < n_steps) {
@@ -830,6 +838,10 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
         bp.src[0].v0 = base + 2 * pl;
         bp.src[0].v1 = base + 3 * pl;
       }
+      if (hooks && hooks->before) {
+        const int rc = hooks->before(t + q);
+        if (rc != MP_OK) return rc;
+      }
       if (tm) cudaEventRecord(tm->ev[0], c->stream);
       e = c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
                  : launch_e_half<T>(ep, c->mode, c->np, c->stream);
@@ -850,6 +862,10 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
         acc[1] += ms[1];  // B half
       }
       c->time++;
+      if (hooks && hooks->after) {
+        const int rc = hooks->after(t + q);
+        if (rc != MP_OK) return rc;
+      }
     }
     t += K;
   }
@@ -1201,6 +1217,78 @@ std::vector<std::pair<void *, size_t>> state_regions(const mp_ctx *c) {
   return r;
 }
 
+// The adjoint face entry per axis of the E (isH false) or H CPML currents: the
+// low and the high face of the axis together (their layers must not overlap,
+// so that a cell is in at most one face per axis).
+template <typename T>
+int adj_faces(mp_ctx *c, DevBufs &buf, bool isH, const CpmlFace<T> *fw, AdjFace<T> out[3]) {
+  const mp_config &g = c->cfg;
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  for (int dim = 0; dim < 3; ++dim) {
+    AdjFace<T> &F = out[dim];
+    F = AdjFace<T>();
+    int fl[2], nf = 0;
+    for (int f = 0; f < 6; ++f) {
+      const LayerHost &L = isH ? c->cpH[f] : c->cpE[f];
+      if (L.active && L.dim == dim && nf < 2) fl[nf++] = f;
+    }
+    if (!nf) continue;
+    const LayerHost *A = isH ? &c->cpH[fl[0]] : &c->cpE[fl[0]];
+    const LayerHost *B = nf == 2 ? (isH ? &c->cpH[fl[1]] : &c->cpE[fl[1]]) : nullptr;
+    int fa = fl[0], fb = nf == 2 ? fl[1] : -1;
+    if (B && B->lo < A->lo) {
+      std::swap(A, B);
+      std::swap(fa, fb);
+    }
+    if (B && B->lo <= A->hi)
+      return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint: the two CPML layers along axis %d overlap", dim);
+    F.active = 1;
+    F.lo0 = A->lo;
+    F.hi0 = A->hi;
+    F.n0 = A->hi - A->lo + 1;
+    F.lo1 = B ? B->lo : 1;
+    F.hi1 = B ? B->hi : 0;
+    const int ntot = F.n0 + (B ? B->hi - B->lo + 1 : 0);
+    F.zlo = A->zlo;
+    F.ex = dim == 0 ? ntot : g.nx;
+    F.ey = dim == 1 ? ntot : g.ny;
+    const size_t zdepth = size_t(g.nz - F.zlo + 1);
+    const size_t cells = dim == 2 ? size_t(ntot) * size_t(c->plane) : zdepth * size_t(F.ex) * size_t(F.ey);
+    void *a0, *a1;
+    cudaError_t e;
+    if ((e = buf.alloc(&a0, cells * sizeof(T))) != cudaSuccess || (e = buf.alloc(&a1, cells * sizeof(T))) != cudaSuccess)
+      return cuda_err(c, e, "adjoint allocation");
+    F.a0 = static_cast<T *>(a0);
+    F.a1 = static_cast<T *>(a1);
+    if (!B) {
+      F.b = fw[fa].b;
+      F.c = fw[fa].c;
+      continue;
+    }
+    // the two faces' b and c lines are zero outside their layers: add them
+    const size_t len = size_t(n3[dim]) + 2;
+    std::vector<T> hb(len), hc(len), tb(len), tc(len);
+    if ((e = cudaMemcpy(hb.data(), fw[fa].b, len * sizeof(T), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(hc.data(), fw[fa].c, len * sizeof(T), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(tb.data(), fw[fb].b, len * sizeof(T), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(tc.data(), fw[fb].c, len * sizeof(T), cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_err(c, e, "line read");
+    for (size_t q = 0; q < len; ++q) {
+      hb[q] += tb[q];
+      hc[q] += tc[q];
+    }
+    void *lb, *lc;
+    if ((e = buf.alloc(&lb, len * sizeof(T))) != cudaSuccess || (e = buf.alloc(&lc, len * sizeof(T))) != cudaSuccess ||
+        (e = cudaMemcpyAsync(lb, hb.data(), len * sizeof(T), cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(lc, hc.data(), len * sizeof(T), cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+      return cuda_err(c, e, "line upload");
+    F.b = static_cast<const T *>(lb);
+    F.c = static_cast<const T *>(lc);
+  }
+  return MP_OK;
+}
+
 int check_objective(mp_ctx *c, const mp_adjoint_config *a) {
   const mp_config &g = c->cfg;
   if (a->kind != MP_OBJ_E2_BOX && a->kind != MP_OBJ_SZ_PLANE)
@@ -1254,12 +1342,11 @@ int objective_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_c
   double *terms;
   cudaError_t e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(a->steps) + 1) * sizeof(double));
   if (e != cudaSuccess) return cuda_err(c, e, "objective allocation");
-  for (long long n = 0; n < a->steps; ++n) {
-    int rc = step_impl<T>(c, ep, bp, 1);
-    if (rc == MP_OK) rc = objective_term<T>(c, a, terms + n);
-    if (rc != MP_OK) return rc;
-  }
-  const int rc = read_sum(c, terms, a->steps, J);
+  StepHooks h;
+  h.after = [&](long long n) { return objective_term<T>(c, a, terms + n); };
+  int rc = step_impl<T>(c, ep, bp, a->steps, nullptr, nullptr, &h);
+  if (rc != MP_OK) return rc;
+  rc = read_sum(c, terms, a->steps, J);
   return rc != MP_OK ? rc : mp_check_status(c);
 }
 
@@ -1325,23 +1412,21 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       if ((e = buf.alloc(&ps, 2 * c->psi_cells * sizeof(T))) != cudaSuccess) return cuda_err(c, e, "adjoint allocation");
       p.psib[s][q] = static_cast<T *>(ps);
     }
-  for (int f = 0; f < 6; ++f)
-    for (int isH = 0; isH < 2; ++isH) {
-      const LayerHost &L = isH ? c->cpH[f] : c->cpE[f];
-      const CpmlFace<T> &F = isH ? bp.cpml[f] : ep.cpml[f];
-      AdjFace<T> &A = isH ? p.fh[f] : p.fe[f];
-      A.active = L.active;
-      if (!L.active) continue;
-      A.dim = L.dim; A.lo = L.lo; A.hi = L.hi; A.zlo = L.zlo; A.ex = L.ex; A.ey = L.ey;
-      A.b = F.b;
-      A.c = F.c;
-      void *a0, *a1;
-      if ((e = buf.alloc(&a0, L.n * sizeof(T))) != cudaSuccess || (e = buf.alloc(&a1, L.n * sizeof(T))) != cudaSuccess)
-        return cuda_err(c, e, "adjoint allocation");
-      A.a0 = static_cast<T *>(a0);
-      A.a1 = static_cast<T *>(a1);
-    }
+  for (int isH = 0; isH < 2; ++isH) {
+    const int rc = adj_faces<T>(c, buf, isH != 0, isH ? bp.cpml : ep.cpml, isH ? p.fh : p.fe);
+    if (rc != MP_OK) return rc;
+  }
   p.nx = g.nx; p.ny = g.ny; p.nz = g.nz;
+  {
+    // planes per block: enough blocks to fill 148 SMs several times over
+    const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+    const long long chunks = std::max(1LL, (148LL * 8 + blocks_xy - 1) / blocks_xy);
+    p.kchunk_e = int(std::max(1LL, (g.nz + chunks - 1) / chunks));
+    p.kchunk_b = int(std::max(1LL, (g.nz + 1 + chunks - 1) / chunks));
+#ifdef MPB_ADJ_KCHUNK
+    p.kchunk_e = p.kchunk_b = MPB_ADJ_KCHUNK;
+#endif
+  }
   p.plane = c->plane;
   p.dt = g.dt;
   for (int q = 0; q < 3; ++q) {
@@ -1360,6 +1445,13 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   p.chi = g.chi;
   p.eps = g.eps;
   p.eps_bg = g.eps_bg;
+  {
+    const double denom0 = c->mode == MODE_PLRC_LIN ? g.eps + (c->sumChi0 - c->sumXi0) : g.eps + c->sumChi0 - c->sumXi0;
+    p.inv_eps_bg = 1.0 / g.eps_bg;
+    p.numer0 = g.eps - c->sumXi0;
+    p.inv_denom0 = 1.0 / denom0;
+    p.A0 = c->mode == MODE_PLRC_NONLIN ? g.chi / denom0 : 0.0;
+  }
   p.np = c->np;
   p.mz0 = c->mz0;
   p.mz1 = c->mz1;
@@ -1382,9 +1474,11 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     }
     return cudaSuccess;
   };
-  auto record = [&](long long slot) -> cudaError_t {
+  // E of a state into a history slot (copied, or, via ep.hist, stored by the E
+  // kernel of the step that produces it); Bx, By on the Sz plane are copied
+  auto record = [&](long long slot, bool withE) -> cudaError_t {
     char *h = hist + size_t(slot) * H;
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < 3 && withE; ++q) {
       cudaError_t err = cudaMemcpyAsync(h + q * fbytes, c->F[q], fbytes, cudaMemcpyDeviceToDevice, c->stream);
       if (err != cudaSuccess) return err;
     }
@@ -1399,21 +1493,46 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   auto slot_e = [&](long long slot, int q) {
     return reinterpret_cast<const T *>(hist + size_t(slot) * H + q * fbytes);
   };
+  auto hist_into = [&](long long slot) {
+    for (int q = 0; q < 3; ++q) ep.hist[q] = slot < 0 ? nullptr : const_cast<T *>(slot_e(slot, q));
+  };
+  // Forward steps n0..n1-1 in one batched call: the E kernel of step n stores
+  // the new E into history slot n + 1 - h0 when n >= h0 (h0 < 0: no history),
+  // the Sz planes are copied after it, and with `objective` the objective term
+  // of step n goes to terms[n].
+  auto forward = [&](long long n0, long long n1, long long h0, bool objective) -> int {
+    StepHooks hk;
+    hk.before = [&](long long q) {
+      const long long n = n0 + q;
+      hist_into(h0 >= 0 && n >= h0 ? n + 1 - h0 : -1);
+      return MP_OK;
+    };
+    hk.after = [&](long long q) {
+      const long long n = n0 + q;
+      if (h0 >= 0 && n >= h0 && sz) {
+        const cudaError_t err = record(n + 1 - h0, false);
+        if (err != cudaSuccess) return cuda_err(c, err, "history copy");
+      }
+      return objective ? objective_term<T>(c, a, terms + n) : MP_OK;
+    };
+    const int r = step_impl<T>(c, ep, bp, int(n1 - n0), nullptr, nullptr, &hk);
+    hist_into(-1);
+    return r;
+  };
   auto slot_b = [&](long long slot, int q) {
     return sz ? reinterpret_cast<const T *>(hist + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
   };
 
   // ---- forward
   const long long t0 = c->time;
-  for (long long n = 0; n < Tn; ++n) {
-    if (n % K == 0 && (e = copy_state(n / K, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
-    if (n >= last0 && (e = record(n - last0)) != cudaSuccess) return cuda_err(c, e, "history copy");
-    int rc = step_impl<T>(c, ep, bp, 1);
-    if (rc == MP_OK) rc = objective_term<T>(c, a, terms + n);
+  for (long long m = 0; m < nseg; ++m) {
+    const long long n0 = m * K, n1 = std::min(n0 + K, Tn);
+    if ((e = copy_state(m, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+    if (n0 == last0 && (e = record(0, true)) != cudaSuccess) return cuda_err(c, e, "history copy");
+    const int rc = forward(n0, n1, n0 == last0 ? last0 : -1, true);
     if (rc != MP_OK) return rc;
   }
-  if ((e = record(Tn - last0)) != cudaSuccess || (e = copy_state(nseg, true)) != cudaSuccess)
-    return cuda_err(c, e, "checkpoint copy");
+  if ((e = copy_state(nseg, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
   int rc = read_sum(c, terms, Tn, J);
   if (rc == MP_OK) rc = mp_check_status(c);
   if (rc != MP_OK) return rc;
@@ -1429,11 +1548,8 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     if (m != nseg - 1) {
       if ((e = copy_state(m, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
       c->time = t0 + n0;
-      for (long long n = n0; n < n1; ++n) {
-        if ((e = record(n - n0)) != cudaSuccess) return cuda_err(c, e, "history copy");
-        if ((rc = step_impl<T>(c, ep, bp, 1)) != MP_OK) return rc;
-      }
-      if ((e = record(n1 - n0)) != cudaSuccess) return cuda_err(c, e, "history copy");
+      if ((e = record(0, true)) != cudaSuccess) return cuda_err(c, e, "history copy");
+      if ((rc = forward(n0, n1, n0, false)) != MP_OK) return rc;
     }
     for (long long n = n1 - 1; n >= n0; --n) {
       for (int q = 0; q < 3; ++q) {

@@ -105,6 +105,7 @@ struct EParams {
 
   CpmlFace<T> cpml[6];    // E-side CPML currents in MPulse's current order
   DesignParams design;
+  T *hist[3];             // with a design region: also store the new E here (adjoint history), if set
   int n_src;
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
@@ -133,15 +134,19 @@ struct BParams {
 // ---------------------------------------------------------------------------
 // Adjoint (mp_adjoint): the discrete adjoint of one PLRC step, run backwards.
 
-// One CPML face's adjoint totals, in the layout of CpmlFace: for an E face the
+// The adjoint totals of the CPML faces along one axis: for an E face the
 // adjoint of its psi after the E half plus dt times the adjoint of the E
 // numerator component it feeds; for an H face the adjoint of its psi after the
-// B half plus dt times the adjoint of the B component it feeds.
+// B half plus dt times the adjoint of the B component it feeds.  The low and
+// the high face of the axis share the entry (their layers must not overlap):
+// positions lo0..hi0 map to 0..n0-1 and lo1..hi1 to n0.. (lo1 > hi1: one
+// face).  Layout like CpmlFace with the merged extent along the axis: z
+// entries [pos][ny][nx]; x entries [k - zlo][ny][ex]; y entries [k - zlo][ey][nx].
 template <typename T>
 struct AdjFace {
-  int active, dim, lo, hi, zlo, ex, ey;
+  int active, lo0, hi0, lo1, hi1, n0, zlo, ex, ey;
   T *a0, *a1;
-  const T *b, *c;
+  const T *b, *c;  // b and c / Delta along the axis (full axis length, both faces)
 };
 
 template <typename T>
@@ -157,8 +162,10 @@ struct AdjParams {
   const T *ikE[3], *ikH[3], *ikH_bzy;
   double pD[3][2], pxi[3][2], pC[3][2];  // active poles, FP64
   double sumChi0, sumXi0, chi, eps, eps_bg;
+  double inv_eps_bg, numer0, inv_denom0, A0;  // background and uniform-medium constants
   int np, mz0, mz1, nonlin;
-  AdjFace<T> fe[6], fh[6];
+  int kchunk_e, kchunk_b;  // planes per block of adj_e (1..nz) / adj_b (0..nz)
+  AdjFace<T> fe[3], fh[3];  // per axis x, y, z
   DesignParams design;
   double *grad[3];        // dJ/d eps, dJ/d Delta-eps factor, dJ/d chi factor (box-sized, FP64)
   // objective term of the state before the step (added when add_obj)

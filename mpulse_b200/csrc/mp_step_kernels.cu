@@ -102,6 +102,11 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
     Ex[base + col] = exn;
     Ey[base + col] = eyn;
     Ez[base + col] = ezn;
+    if (DESIGN && p.hist[0]) {
+      p.hist[0][base + col] = exn;
+      p.hist[1][base + col] = eyn;
+      p.hist[2][base + col] = ezn;
+    }
     if (NP > 0 && med) {
 #pragma unroll
       for (int n = 0; n < NP; ++n)

@@ -237,6 +237,7 @@ def run_ours(args) -> dict:
 
     # end to end through the C ABI with host buffers
     e2e = run_e2e(args, torch, stream, local_rank)
+    adjoint = run_adjoint(local_rank) if rank == 0 else None
 
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -249,7 +250,8 @@ def run_ours(args) -> dict:
         "fp64": {"value": round(value64, 4), "unit": UNIT, "ms_per_step": round(dt64 / args.steps * 1e3, 4)},
         "fp32_over_fp64": round(value / value64, 3) if value64 > 0 else None,
         "rel_l2_fp32_vs_fp64": rel,
-        "adjoint_forward_ratio": None,
+        "adjoint_forward_ratio": adjoint["fp32"]["ratio"] if adjoint else None,
+        "adjoint": adjoint,
         "roofline": roofline, "step_roofline": step_roofline,
         "kernel_ms": kt,
         "e2e": e2e,
@@ -262,6 +264,55 @@ def run_ours(args) -> dict:
         dist.barrier()
         dist.destroy_process_group()
     return out if rank == 0 else None
+
+
+def run_adjoint(local_rank: int) -> dict:
+    """The adjoint workload (96^3, single-pole medium, 32^3 design region,
+    1500 steps, |E|^2 monitor objective): wall time of the forward run that
+    computes J (mp_objective) and of mp_adjoint (forward with checkpoints +
+    reverse pass), best of two; FP32 with a checkpoint every 50 steps (the
+    workload's schedule) and with the whole E history kept, and the FP32
+    gradient against the FP64 one."""
+    from mpulse_b200 import runtime
+
+    out = {"workload": "adjoint_plrc_96^3_design32^3_1500steps", "unit": "s"}
+    grads = {}
+    for prec, tag in ((abi.MP_FP32, "fp32"), (abi.MP_FP64, "fp64")):
+        cfg, des, adj = configs.c4_adjoint(prec)
+        cfg.device = local_rank
+        full = abi.adjoint_config(adj.kind, list(adj.box), adj.steps, checkpoint_every=adj.steps)
+
+        def fresh():
+            g = runtime.Simulation(cfg)
+            for k, v in des.items():
+                g.upload_design(k, v)
+            g.sync()
+            return g
+
+        def timed(fn):
+            best, res = None, None
+            for _ in range(2):
+                with fresh() as g:
+                    t0 = time.perf_counter()
+                    res = fn(g)
+                    t = time.perf_counter() - t0
+                best = t if best is None else min(best, t)
+            return best, res
+
+        warm = abi.adjoint_config(adj.kind, list(adj.box), 60, checkpoint_every=20)
+        with fresh() as g:
+            g.adjoint(warm)
+        fwd, J = timed(lambda g: g.objective(adj))
+        t_adj, (Ja, gr) = timed(lambda g: g.adjoint(adj))
+        t_full, _ = timed(lambda g: g.adjoint(full))
+        grads[tag] = gr["DesignEps"]
+        out[tag] = {"forward_s": round(fwd, 4), "adjoint_s": round(t_adj, 4),
+                    "ratio": round(t_adj / fwd, 3), "checkpoint_every": adj.checkpoint_every,
+                    "adjoint_full_history_s": round(t_full, 4), "ratio_full_history": round(t_full / fwd, 3),
+                    "J": J}
+    g32, g64 = grads["fp32"], grads["fp64"]
+    out["grad_rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    return out
 
 
 def run_profile(args) -> dict:

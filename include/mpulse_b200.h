@@ -134,7 +134,10 @@ typedef struct mp_source {
   double width;      /* plane_gauss_inject width (default 10) */
   double offset;     /* plane_gauss_inject offset (default 40) */
   double eps;        /* background permittivity of the source (default 1) */
-  /* short_pulse_inject / focused_pulse_inject (shortpulseinject.cpp:33-49) */
+  /* short_pulse_inject (shortpulseinject.cpp:33-49).  focused_pulse_inject
+   * takes the same keys (focusedpulseinject.cpp:39-57); its plug-in does not
+   * compile in MPulse, and here it is defined as the same paraxial closed form
+   * injected on the down face (OversampleX/Y have no meaning for it). */
   double length;     /* pulse duration parameter T */
   double waist;      /* "width": beam waist w0 */
   double om0;        /* carrier frequency (default 2 pi) */

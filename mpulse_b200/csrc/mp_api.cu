@@ -214,8 +214,6 @@ int validate(const mp_config *c) {
   if (c->n_sources < 0 || c->n_sources > MP_MAX_SOURCES) return set_err(nullptr, MP_ERR_INVALID, "n_sources out of range");
   for (int s = 0; s < c->n_sources; ++s) {
     const mp_source &q = c->sources[s];
-    if (q.kind == MP_SOURCE_FOCUSED_PULSE)
-      return set_err(nullptr, MP_ERR_UNSUPPORTED, "focused_pulse_inject is not built");
     if (q.kind < MP_SOURCE_PLANE_WAVE || q.kind > MP_SOURCE_GAUSS_BEAM)
       return set_err(nullptr, MP_ERR_INVALID, "source %d: unknown kind %d", s, q.kind);
     if (q.kind == MP_SOURCE_GAUSS_BEAM && (q.t_size < 1 || q.t_size > (1 << 22)))
@@ -1350,12 +1348,117 @@ int objective_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_c
   return rc != MP_OK ? rc : mp_check_status(c);
 }
 
-// Forward with checkpoints, then the reverse pass segment by segment: a
-// segment [n0, n1) is recomputed from its checkpoint keeping E (and, for the Sz
-// objective, Bx and By on the plane) of every state n0..n1, then stepped back
-// with adj_e / adj_b from n1 - 1 down to n0.  The last segment's history is
-// kept during the first forward run, so with one segment nothing is
-// recomputed.
+// The checkpoint schedule of the reverse pass.  The steps are cut into chunks
+// of Kh steps whose E history fits the history buffer; a chunk is reversed by
+// running it forward from its start keeping E of every step ("leaf") and then
+// stepping back.  Chunk starts are kept as state checkpoints where slots allow,
+// placed by the binomial rule of revolve (Griewank): with s free slots and r
+// the smallest number of sweeps with C(s + r, s) >= m chunks, the next
+// checkpoint leaves C(s + r - 1, s) chunks to its left; with no free slot left
+// the chunks are run again from the last checkpoint, last chunk first.
+struct RevolveOps {
+  std::function<int(long long, int)> restore;    // live state := checkpoint slot, at step
+  std::function<int(long long, int)> save;       // checkpoint slot := live state
+  std::function<int(long long, long long)> advance;  // run from -> to, no history
+  std::function<int(long long, long long)> leaf;     // live at n0: run n0 -> n1 keeping E, step back
+};
+
+double binom_sr(int s, int r) {  // C(s + r, s)
+  double v = 1;
+  for (int q = 1; q <= s; ++q) v = v * double(r + q) / double(q);
+  return v;
+}
+
+int revolve(long long a, long long b, int slot_a, std::vector<int> &free_slots, long long Kh, RevolveOps &ops,
+            long long &live) {
+  int rc;
+  const long long m = (b - a + Kh - 1) / Kh;
+  if (m <= 1) {
+    if (live != a && (rc = ops.restore(a, slot_a)) != MP_OK) return rc;
+    if ((rc = ops.leaf(a, b)) != MP_OK) return rc;
+    live = b;
+    return MP_OK;
+  }
+  if (free_slots.empty()) {
+    for (long long e = b; e > a;) {
+      const long long c0 = std::max(a, e - Kh);
+      if (live != a && (rc = ops.restore(a, slot_a)) != MP_OK) return rc;
+      live = a;
+      if (c0 > a && (rc = ops.advance(a, c0)) != MP_OK) return rc;
+      if ((rc = ops.leaf(c0, e)) != MP_OK) return rc;
+      live = e;
+      e = c0;
+    }
+    return MP_OK;
+  }
+  const int s = int(free_slots.size());
+  int r = 1;
+  while (binom_sr(s, r) < double(m)) ++r;
+  const long long left = std::max(1LL, std::min(m - 1, (long long)binom_sr(s, r - 1)));
+  const long long cpos = a + left * Kh;
+  if (live != a && (rc = ops.restore(a, slot_a)) != MP_OK) return rc;
+  if ((rc = ops.advance(a, cpos)) != MP_OK) return rc;
+  live = cpos;
+  const int sc = free_slots.back();
+  free_slots.pop_back();
+  if ((rc = ops.save(cpos, sc)) != MP_OK) return rc;
+  if ((rc = revolve(cpos, b, sc, free_slots, Kh, ops, live)) != MP_OK) return rc;
+  free_slots.push_back(sc);
+  return revolve(a, cpos, slot_a, free_slots, Kh, ops, live);
+}
+
+// Steps the schedule runs forward in all (first pass and recomputation).
+long long schedule_steps(long long Tn, long long Kh, int slots) {
+  long long steps = 0;
+  RevolveOps ops;
+  ops.restore = [](long long, int) { return MP_OK; };
+  ops.save = [](long long, int) { return MP_OK; };
+  ops.advance = [&](long long f, long long t) { steps += t - f; return MP_OK; };
+  ops.leaf = [&](long long f, long long t) { steps += t - f; return MP_OK; };
+  std::vector<int> free_slots;
+  for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+  long long live = 0;
+  revolve(0, Tn, 0, free_slots, Kh, ops, live);
+  return steps;
+}
+
+// History chunk Kh and checkpoint slots for Tn steps: checkpoint_every K > 0
+// gives chunks of K with a checkpoint at every chunk start; a memory budget
+// (bytes for (slots + 1) states and Kh + 1 steps of history) gives the plan
+// with the fewest forward steps; neither keeps the whole history.
+bool plan_schedule(long long Tn, long long every, double budget, size_t S, size_t H, long long *Kh, int *slots) {
+  if (every > 0) {
+    *Kh = std::min(every, Tn);
+    *slots = int((Tn + *Kh - 1) / *Kh);
+    return true;
+  }
+  if (!(budget > 0)) {
+    *Kh = Tn;
+    *slots = 1;
+    return true;
+  }
+  long long best = -1;
+  for (long long kh = Tn; kh >= 1; kh = std::min(kh - 1, (long long)(kh * 0.9))) {
+    const double room = budget - double(kh + 1) * double(H) - double(S);  // one slot for the final state
+    if (room < double(S)) continue;
+    const long long m = (Tn + kh - 1) / kh;
+    const int s = int(std::min<double>(double(m), std::floor(room / double(S))));
+    const long long cost = schedule_steps(Tn, kh, s);
+    if (best < 0 || cost < best) {
+      best = cost;
+      *Kh = kh;
+      *slots = s;
+    }
+  }
+  return best >= 0;
+}
+
+// The forward run and the reverse pass on the schedule of plan_schedule /
+// revolve: each chunk [n0, n1) is run forward from the live state or a
+// checkpoint keeping E (and, for the Sz objective, Bx and By on the plane) of
+// every state n0..n1, then stepped back with adj_e / adj_b from n1 - 1 down to
+// n0.  The last chunk is reversed straight after the first run reaches it, so
+// with one chunk nothing is recomputed.
 template <typename T>
 int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_config *a, double *J, double *gout[3]) {
   const mp_config &g = c->cfg;
@@ -1366,30 +1469,19 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   const bool sz = a->kind == MP_OBJ_SZ_PLANE;
   const size_t fbytes = c->fcount * sizeof(T), pbytes = size_t(c->plane) * sizeof(T);
   const size_t H = 3 * fbytes + (sz ? 2 * pbytes : 0);
-  long long K = a->checkpoint_every;
-  if (K <= 0) {
-    if (!(a->mem_budget > 0)) {
-      K = Tn;
-    } else {
-      K = 0;
-      for (long long k = Tn; k >= 1 && !K; --k) {
-        const long long nseg = (Tn + k - 1) / k;
-        if (double(nseg + 1) * double(S) + double(k + 1) * double(H) <= a->mem_budget) K = k;
-      }
-      if (!K)
-        return set_err(c, MP_ERR_NO_MEMORY,
-                       "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
-                       a->mem_budget, S, H);
-    }
-  }
-  K = std::min(K, Tn);
-  const long long nseg = (Tn + K - 1) / K, last0 = (nseg - 1) * K;
+  long long Kh = 0;  // steps per history chunk
+  int slots = 0;     // state checkpoints (the initial state included)
+  if (!plan_schedule(Tn, a->checkpoint_every, a->mem_budget, S, H, &Kh, &slots))
+    return set_err(c, MP_ERR_NO_MEMORY,
+                   "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
+                   a->mem_budget, S, H);
+  const long long K = Kh;
 
   DevBufs buf(c->stream);
   cudaError_t e;
   char *ckpt, *hist;
   double *terms;
-  if ((e = buf.alloc(reinterpret_cast<void **>(&ckpt), size_t(nseg + 1) * S)) != cudaSuccess ||
+  if ((e = buf.alloc(reinterpret_cast<void **>(&ckpt), size_t(slots + 1) * S)) != cudaSuccess ||
       (e = buf.alloc(reinterpret_cast<void **>(&hist), size_t(K + 1) * H)) != cudaSuccess ||
       (e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(Tn) + 1) * sizeof(double))) != cudaSuccess)
     return cuda_err(c, e, "checkpoint allocation");
@@ -1493,14 +1585,21 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   auto slot_e = [&](long long slot, int q) {
     return reinterpret_cast<const T *>(hist + size_t(slot) * H + q * fbytes);
   };
+  auto slot_b = [&](long long slot, int q) {
+    return sz ? reinterpret_cast<const T *>(hist + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
+  };
   auto hist_into = [&](long long slot) {
     for (int q = 0; q < 3; ++q) ep.hist[q] = slot < 0 ? nullptr : const_cast<T *>(slot_e(slot, q));
   };
-  // Forward steps n0..n1-1 in one batched call: the E kernel of step n stores
-  // the new E into history slot n + 1 - h0 when n >= h0 (h0 < 0: no history),
-  // the Sz planes are copied after it, and with `objective` the objective term
-  // of step n goes to terms[n].
-  auto forward = [&](long long n0, long long n1, long long h0, bool objective) -> int {
+  // ---- forward and reverse on the checkpoint schedule
+  const long long t0 = c->time;
+  long long reached = 0;  // steps whose objective term is computed
+  bool at_end = false;
+  // Forward steps n0..n1-1 from the live state in one batched call: the E
+  // kernel of step n stores the new E into history slot n + 1 - h0 when
+  // n >= h0 (h0 < 0: no history), the Sz planes are copied after it, and the
+  // objective term of every step not run before goes to terms[n].
+  auto run = [&](long long n0, long long n1, long long h0) -> int {
     StepHooks hk;
     hk.before = [&](long long q) {
       const long long n = n0 + q;
@@ -1513,43 +1612,39 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
         const cudaError_t err = record(n + 1 - h0, false);
         if (err != cudaSuccess) return cuda_err(c, err, "history copy");
       }
-      return objective ? objective_term<T>(c, a, terms + n) : MP_OK;
+      return n >= reached ? objective_term<T>(c, a, terms + n) : MP_OK;
     };
     const int r = step_impl<T>(c, ep, bp, int(n1 - n0), nullptr, nullptr, &hk);
     hist_into(-1);
+    reached = std::max(reached, n1);
     return r;
   };
-  auto slot_b = [&](long long slot, int q) {
-    return sz ? reinterpret_cast<const T *>(hist + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
+  RevolveOps ops;
+  ops.restore = [&](long long at, int slot) {
+    const cudaError_t err = copy_state(slot, false);
+    c->time = t0 + at;
+    return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint restore");
   };
-
-  // ---- forward
-  const long long t0 = c->time;
-  for (long long m = 0; m < nseg; ++m) {
-    const long long n0 = m * K, n1 = std::min(n0 + K, Tn);
-    if ((e = copy_state(m, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
-    if (n0 == last0 && (e = record(0, true)) != cudaSuccess) return cuda_err(c, e, "history copy");
-    const int rc = forward(n0, n1, n0 == last0 ? last0 : -1, true);
-    if (rc != MP_OK) return rc;
-  }
-  if ((e = copy_state(nseg, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
-  int rc = read_sum(c, terms, Tn, J);
-  if (rc == MP_OK) rc = mp_check_status(c);
-  if (rc != MP_OK) return rc;
-
-  // ---- reverse
-  for (int q = 0; q < 3; ++q) p.En[q] = slot_e(Tn - last0, q);
-  p.obx = slot_b(Tn - last0, 0);
-  p.oby = slot_b(Tn - last0, 1);
-  if ((e = launch_adj_init<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint init kernel");
-  c->launches++;
-  for (long long m = nseg - 1; m >= 0; --m) {
-    const long long n0 = m * K, n1 = std::min(n0 + K, Tn);
-    if (m != nseg - 1) {
-      if ((e = copy_state(m, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
-      c->time = t0 + n0;
-      if ((e = record(0, true)) != cudaSuccess) return cuda_err(c, e, "history copy");
-      if ((rc = forward(n0, n1, n0, false)) != MP_OK) return rc;
+  ops.save = [&](long long, int slot) {
+    const cudaError_t err = copy_state(slot, true);
+    return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint copy");
+  };
+  ops.advance = [&](long long from, long long to) { return run(from, to, -1); };
+  ops.leaf = [&](long long n0, long long n1) -> int {
+    cudaError_t err;
+    if ((err = record(0, true)) != cudaSuccess) return cuda_err(c, err, "history copy");
+    int r = run(n0, n1, n0);
+    if (r != MP_OK) return r;
+    if (n1 == Tn && !at_end) {
+      // the first time the run reaches the end: J, the final state, the start of the adjoint
+      at_end = true;
+      if ((err = copy_state(slots, true)) != cudaSuccess) return cuda_err(c, err, "checkpoint copy");
+      if ((r = read_sum(c, terms, Tn, J)) != MP_OK || (r = mp_check_status(c)) != MP_OK) return r;
+      for (int q = 0; q < 3; ++q) p.En[q] = slot_e(n1 - n0, q);
+      p.obx = slot_b(n1 - n0, 0);
+      p.oby = slot_b(n1 - n0, 1);
+      if ((err = launch_adj_init<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint init kernel");
+      c->launches++;
     }
     for (long long n = n1 - 1; n >= n0; --n) {
       for (int q = 0; q < 3; ++q) {
@@ -1559,12 +1654,19 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       p.obx = slot_b(n - n0, 0);
       p.oby = slot_b(n - n0, 1);
       p.add_obj = n >= 1;
-      if ((e = launch_adj_e<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint E kernel");
-      if ((e = launch_adj_b<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, e, "adjoint B kernel");
+      if ((err = launch_adj_e<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint E kernel");
+      if ((err = launch_adj_b<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint B kernel");
       c->launches += 2;
     }
-  }
-  if ((e = copy_state(nseg, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
+    return MP_OK;
+  };
+  if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+  std::vector<int> free_slots;
+  for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+  long long live = 0;
+  int rc = revolve(0, Tn, 0, free_slots, K, ops, live);
+  if (rc != MP_OK) return rc;
+  if ((e = copy_state(slots, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
   c->time = t0 + Tn;
   for (int q = 0; q < 3; ++q)
     if (gout[q] && (e = cudaMemcpyAsync(gout[q], p.grad[q], c->dcells * sizeof(double), cudaMemcpyDeviceToHost,

@@ -81,7 +81,7 @@ __device__ void gauss_beam_field(const SourceEvalParams &q, int i, int j, double
 
 // The incident field at interior column (i, j) (0-based; MPulse i + 1, j + 1).
 __device__ void source_field(const SourceEvalParams &q, int i, int j, double f[3]) {
-  if (q.kind == 3) short_pulse_field(q, i + 1, j + 1, q.l, f);
+  if (q.kind == 3 || q.kind == 4) short_pulse_field(q, i + 1, j + 1, q.l, f);  // short / focused pulse
   else if (q.kind == 5) gauss_beam_field(q, i, j, f);
   else plane_source_field(q, i + 1, j + 1, q.l, f);
 }

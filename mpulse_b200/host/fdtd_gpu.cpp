@@ -55,7 +55,7 @@ ParameterMap *GpuSourceBlock::MakeParamMap(ParameterMap *pm) {
     (*pm)["width"] = WParameter(new ParameterValue<double>(&width, 10));
     (*pm)["offset"] = WParameter(new ParameterValue<double>(&offset, 40));
   }
-  if (kind == MP_SOURCE_SHORT_PULSE) {
+  if (kind == MP_SOURCE_SHORT_PULSE || kind == MP_SOURCE_FOCUSED_PULSE) {
     (*pm)["length"] = WParameter(new ParameterValue<double>(&length, 1.));
     (*pm)["width"] = WParameter(new ParameterValue<double>(&waist, 1.));
     (*pm)["om0"] = WParameter(new ParameterValue<double>(&om0, 2 * M_PI));
@@ -64,6 +64,12 @@ ParameterMap *GpuSourceBlock::MakeParamMap(ParameterMap *pm) {
     (*pm)["Phase"] = WParameter(new ParameterValue<double>(&Phase, 0));
     (*pm)["amp"] = WParameter(new ParameterValue<double>(&amp, 1));
     (*pm)["eps"] = WParameter(new ParameterValue<double>(&eps, 1));
+  }
+  if (kind == MP_SOURCE_FOCUSED_PULSE) {
+    // FocusedPulseInject::MakeParamMap (focusedpulseinject.cpp:39-57): the
+    // angular-spectrum oversampling has no meaning for the closed form
+    (*pm)["OversampleX"] = WParameter(new ParameterValue<int>(&oversampleX, 1));
+    (*pm)["OversampleY"] = WParameter(new ParameterValue<int>(&oversampleY, 1));
   }
   if (kind == MP_SOURCE_GAUSS_BEAM) {  // GaussInject::MakeParamMap (gaussinject.cpp:33-49)
     (*pm)["SizeT"] = WParameter(new ParameterValue<int>(&SizeT, 4096));
@@ -96,7 +102,7 @@ void GpuSourceBlock::fill(mp_source &s) const {
     s.width = width;
     s.offset = offset;
   }
-  if (kind == MP_SOURCE_SHORT_PULSE) {
+  if (kind == MP_SOURCE_SHORT_PULSE || kind == MP_SOURCE_FOCUSED_PULSE) {
     s.length = length; s.waist = waist; s.om0 = om0;
     s.t_shift = TShift; s.z_shift = ZShift; s.phase = Phase; s.amp = amp; s.eps = eps;
   }
@@ -146,6 +152,8 @@ ParameterMap *FDTD_GPU::MakeParamMap(ParameterMap *pm) {
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_SHORT_PULSE>, CurrentFactory>(&blocks));
   (*pm)["gauss_inject"] =
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_GAUSS_BEAM>, CurrentFactory>(&blocks));
+  (*pm)["focused_pulse_inject"] =
+      WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_FOCUSED_PULSE>, CurrentFactory>(&blocks));
   return pm;
 }
 

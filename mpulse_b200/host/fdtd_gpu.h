@@ -64,6 +64,7 @@ class GpuSourceBlock : public CurrentFactory {
   double ramp, width, offset, eps;
   double length, waist, om0, TShift, ZShift, Phase, amp;
   int SizeT, toff;
+  int oversampleX, oversampleY;  // focused_pulse_inject keys, read and not used
   double k0, Shift, Time;
   void fill(mp_source &s) const;
 

@@ -492,7 +492,7 @@ static void src_hfield(const mpo_sim *s, int n, int i, int j, int l, long long t
     }
     return;
   }
-  if (p->kind == MP_SOURCE_SHORT_PULSE) {
+  if (p->kind == MP_SOURCE_SHORT_PULSE || p->kind == MP_SOURCE_FOCUSED_PULSE) {
     /* ShortPulseInjectSourceFunc::getHField (shortpulseinject.cpp:151-178) */
     const double posxo = (i - st->centre[0]) * dx;
     const double posxh = (i + 0.5 - st->centre[0]) * dx;
@@ -543,7 +543,7 @@ static void src_efield(const mpo_sim *s, int n, int i, int j, int l, long long t
     }
     return;
   }
-  if (p->kind == MP_SOURCE_SHORT_PULSE) {
+  if (p->kind == MP_SOURCE_SHORT_PULSE || p->kind == MP_SOURCE_FOCUSED_PULSE) {
     const double posxh = (i + 0.5 - st->centre[0]) * dx;
     const double posyo = (j - st->centre[1]) * dy;
     const double poszo = (l - st->centre[2]) * dz - st->zshift;
@@ -1188,8 +1188,10 @@ int mpo_create(const mp_config *cfg, mpo_sim **out) {
       const double factor = -bmag / sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
       for (int c = 0; c < 3; ++c) st->E[c] = E[c] * (factor / sqrt(p->eps));
       st->om = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]) / sqrt(p->eps);
-    } else if (p->kind == MP_SOURCE_SHORT_PULSE) {
-      /* ShortPulseInjectSourceFunc::setParam (shortpulseinject.cpp:56-113) */
+    } else if (p->kind == MP_SOURCE_SHORT_PULSE || p->kind == MP_SOURCE_FOCUSED_PULSE) {
+      /* ShortPulseInjectSourceFunc::setParam (shortpulseinject.cpp:56-113); the
+       * focused pulse is defined as the same closed form (its reference plug-in,
+       * focusedpulseinject.cpp, does not compile) */
       st->centre[0] = 0.5 * (double)(cfg->nx + 1);
       st->centre[1] = 0.5 * (double)(cfg->ny + 1);
       st->centre[2] = 0.5 * (double)(cfg->nz + 1);

@@ -109,25 +109,33 @@ def test_fp64_adjoint_matches_restatement(solver, kind, every):
         assert rel_l2(grads[name], ref) <= 1e-10, (name, rel_l2(grads[name], ref))
 
 
-def test_adjoint_memory_budget_schedule():
-    """A budget that holds only a few states gives short segments and the same
-    gradient; one too small to hold a schedule is refused."""
+@pytest.mark.parametrize("per_cell", [864.0, 648.0, 516.0])
+def test_adjoint_memory_budget_schedule(per_cell):
+    """Budgets that hold only a few states give the same J and gradient as the
+    whole history: one state is about 8 B x cells x (6 fields + 2 poles x 3
+    components x 2 x 11/16 medium planes) plus the CPML psi (~126 B per cell),
+    one step of history 24 B per cell.  864 B per cell: two checkpoints; 648:
+    three slots for six chunks (binomial placement, chunks run up to three
+    times); 516: one slot, every chunk run again from the start."""
     cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
     des = design_maps(cfg, 18)
     init = clean_init(cfg, 19, smooth=True, scale=0.2)
     full = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], 30)
     with gpu_sim(cfg, init, des) as g:
         J0, g0 = g.adjoint(full)
-    # one state is about 8 B x cells x (6 fields + 2 poles x 3 components x 2 x
-    # 11/16 medium planes) plus the CPML psi, one step of history 8 B x 3 x cells;
-    # 864 B per cell holds two segments ([0, 19), [19, 30)) but not one
-    tight = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], 30, mem_budget=864.0 * cfg.field_count())
+    tight = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], 30,
+                               mem_budget=per_cell * cfg.field_count())
     with gpu_sim(cfg, init, des) as g:
         J1, g1 = g.adjoint(tight)
+        assert g.time == 30
     assert abs(J1 - J0) <= 1e-14 * abs(J0)
     for name in abi.DESIGN_NAMES[:2]:
         assert rel_l2(g1[name], g0[name]) <= 1e-13
-    with gpu_sim(cfg, init, des) as g:
+
+
+def test_adjoint_memory_budget_too_small():
+    cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
+    with gpu_sim(cfg, {}, {}) as g:
         with pytest.raises(runtime.MPulseError):
             g.adjoint(abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], 30, mem_budget=1000.0))
 

@@ -315,6 +315,25 @@ def run_adjoint(local_rank: int) -> dict:
     return out
 
 
+def run_adjoint_profile(args) -> dict:
+    """The adjoint workload only, FP32, args.steps steps with a checkpoint
+    every args.checkpoint steps: mp_objective, then mp_adjoint (for ncu
+    captures of the adjoint kernels)."""
+    from mpulse_b200 import runtime
+    cfg, des, adj = configs.c4_adjoint(abi.MP_FP32)
+    a = abi.adjoint_config(adj.kind, list(adj.box), args.steps, checkpoint_every=args.checkpoint)
+    out = {"adjoint_profile_run": True, "steps": args.steps, "checkpoint_every": args.checkpoint}
+    with runtime.Simulation(cfg) as g:
+        for k, v in des.items():
+            g.upload_design(k, v)
+        out["J_objective"] = g.objective(a)
+    with runtime.Simulation(cfg) as g:
+        for k, v in des.items():
+            g.upload_design(k, v)
+        out["J_adjoint"], _ = g.adjoint(a)
+    return out
+
+
 def run_profile(args) -> dict:
     """FP32 workload only: warm-up, then the timed steps; no other kernels."""
     import torch
@@ -467,12 +486,17 @@ def main():
     ap.add_argument("--profile-only", action="store_true",
                     help="only the FP32 warm-up and timed steps (for ncu captures)")
     ap.add_argument("--nz", type=int, default=None, help="override nz (smaller case for ncu --set full)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="only mp_objective + mp_adjoint of the adjoint workload for --steps steps (ncu captures)")
+    ap.add_argument("--checkpoint", type=int, default=50, help="checkpoint interval of --adjoint-only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.nz:
         WORKLOAD["nz"] = args.nz
-    if args.profile_only:
+    if args.adjoint_only:
+        out = run_adjoint_profile(args)
+    elif args.profile_only:
         out = run_profile(args)
     else:
         out = run_reference_arm(args) if args.impl == "reference" else run_ours(args)

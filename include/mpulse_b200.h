@@ -334,6 +334,16 @@ long long mp_launch_count(mp_ctx *ctx);
 int mp_kernel_times(mp_ctx *ctx, int n_steps, double *e_half_ms, double *b_half_ms,
                     double *sources_ms);
 
+/* Checkpoint / restart of the whole device state: the six fields, the PLRC
+ * accumulators, the CPML psi of every face and the time (the injector state
+ * is a function of the time).  The buffer is opaque, in the device precision,
+ * with a header that mp_load_state checks against the context (grid,
+ * precision, solver, boundary, CPML, medium planes).  MPulse itself has no
+ * restart (Globals::IsRestart is never read, src/globals.h:45,90-92). */
+int mp_state_size(mp_ctx *ctx, size_t *bytes);
+int mp_save_state(mp_ctx *ctx, void *host, size_t bytes);
+int mp_load_state(mp_ctx *ctx, const void *host, size_t bytes);
+
 /* Runs adj->steps steps like mp_step and returns the objective J of adj over
  * them in *J (FP64 accumulation).  No counterpart in MPulse. */
 int mp_objective(mp_ctx *ctx, const mp_adjoint_config *adj, double *J);

@@ -1705,3 +1705,93 @@ int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_ep
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// mp_state_size / mp_save_state / mp_load_state
+
+namespace {
+
+struct StateHeader {
+  char magic[8];  // "MPB200ST"
+  int abi_version, precision, solver, boundary, cpml, cpml_d;
+  int nx, ny, nz, mz0, mz1, np, nregions;
+  long long time;
+  unsigned long long payload;
+};
+
+void fill_header(const mp_ctx *c, const std::vector<std::pair<void *, size_t>> &regions, StateHeader &h) {
+  memset(&h, 0, sizeof h);
+  memcpy(h.magic, "MPB200ST", 8);
+  h.abi_version = MP_ABI_VERSION;
+  h.precision = c->cfg.precision;
+  h.solver = c->cfg.solver;
+  h.boundary = c->cfg.boundary;
+  h.cpml = c->cfg.cpml;
+  h.cpml_d = c->cfg.cpml_d;
+  h.nx = c->cfg.nx;
+  h.ny = c->cfg.ny;
+  h.nz = c->cfg.nz;
+  h.mz0 = c->mz0;
+  h.mz1 = c->mz1;
+  h.np = c->np;
+  h.nregions = int(regions.size());
+  h.time = c->time;
+  for (const auto &r : regions) h.payload += r.second;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_state_size(mp_ctx *c, size_t *bytes) {
+  if (!c || !bytes) return MP_ERR_INVALID;
+  StateHeader h;
+  fill_header(c, state_regions(c), h);
+  *bytes = sizeof(StateHeader) + size_t(h.payload);
+  return MP_OK;
+}
+
+int mp_save_state(mp_ctx *c, void *host, size_t bytes) {
+  if (!c || !host) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  const auto regions = state_regions(c);
+  StateHeader h;
+  fill_header(c, regions, h);
+  if (bytes != sizeof h + size_t(h.payload))
+    return set_err(c, MP_ERR_INVALID, "state buffer of %zu bytes, expected %zu", bytes, sizeof h + size_t(h.payload));
+  memcpy(host, &h, sizeof h);
+  char *dst = static_cast<char *>(host) + sizeof h;
+  for (const auto &r : regions) {
+    cudaError_t e = cudaMemcpyAsync(dst, r.first, r.second, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "state copy");
+    dst += r.second;
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? MP_OK : cuda_err(c, e, "state copy");
+}
+
+int mp_load_state(mp_ctx *c, const void *host, size_t bytes) {
+  if (!c || !host) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  const auto regions = state_regions(c);
+  StateHeader want, got;
+  fill_header(c, regions, want);
+  if (bytes < sizeof got) return set_err(c, MP_ERR_INVALID, "state buffer too short");
+  memcpy(&got, host, sizeof got);
+  want.time = got.time;
+  if (memcmp(&want, &got, sizeof got) != 0 || bytes != sizeof got + size_t(got.payload))
+    return set_err(c, MP_ERR_INVALID, "state buffer does not match this context (grid, precision, solver, "
+                                      "boundary, CPML or medium differ)");
+  const char *src = static_cast<const char *>(host) + sizeof got;
+  for (const auto &r : regions) {
+    cudaError_t e = cudaMemcpyAsync(r.first, src, r.second, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "state copy");
+    src += r.second;
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "state copy");
+  c->time = got.time;
+  return MP_OK;
+}
+
+}  // extern "C"

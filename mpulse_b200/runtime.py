@@ -25,7 +25,8 @@ EXPORTED = (
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
-    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint",
+    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_state_size", "mp_save_state",
+    "mp_load_state",
 )
 
 _lib = None
@@ -88,6 +89,12 @@ def lib():
     L.mp_objective.restype = C.c_int
     L.mp_adjoint.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp, dp, dp, dp]
     L.mp_adjoint.restype = C.c_int
+    L.mp_state_size.argtypes = [vp, C.POINTER(sz)]
+    L.mp_state_size.restype = C.c_int
+    L.mp_save_state.argtypes = [vp, vp, sz]
+    L.mp_save_state.restype = C.c_int
+    L.mp_load_state.argtypes = [vp, vp, sz]
+    L.mp_load_state.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
@@ -226,3 +233,16 @@ class Simulation:
         J = C.c_double()
         self._check(lib().mp_adjoint(self._h, C.byref(adj), C.byref(J), _dptr(g[0]), _dptr(g[1]), _dptr(g[2])))
         return J.value, {name: a.reshape(shape) for name, a in zip(abi.DESIGN_NAMES, g)}
+
+    # -- checkpoint / restart
+    def save_state(self) -> bytes:
+        """The whole device state and the time (mp_save_state)."""
+        n = C.c_size_t()
+        self._check(lib().mp_state_size(self._h, C.byref(n)))
+        buf = (C.c_char * n.value)()
+        self._check(lib().mp_save_state(self._h, buf, n.value))
+        return bytes(buf)
+
+    def load_state(self, data: bytes):
+        buf = C.create_string_buffer(data, len(data))
+        self._check(lib().mp_load_state(self._h, buf, len(data)))

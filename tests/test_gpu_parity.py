@@ -183,3 +183,33 @@ def test_tma_kernels_match_oracle(case):
     got, want = run_pair(cfg, init, STEPS)
     for n in abi.FIELD_NAMES:
         assert rel_l2(got[n], want[n]) <= TOL_FP64, n
+
+
+@pytest.mark.parametrize("case", ["nonlin_all_short", "lin_cpmlz_gauss_beam", "nonlin_three_poles"])
+def test_save_and_load_state_resumes_bit_for_bit(case):
+    """mp_save_state / mp_load_state: a run resumed from a saved state, in the
+    same context or a new one, continues exactly like the uninterrupted run."""
+    cfg = make_case(case, abi.MP_FP32)
+    init = random_fields(cfg, seed=5, smooth=True)
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.step(7)
+        snap = g.save_state()
+        g.step(9)
+        want = {n: g.download(n) for n in abi.FIELD_NAMES}
+        g.step(3)
+        g.load_state(snap)
+        assert g.time == 7
+        g.step(9)
+        for n in abi.FIELD_NAMES:
+            np.testing.assert_array_equal(g.download(n), want[n])
+    with runtime.Simulation(cfg) as h:
+        h.load_state(snap)
+        h.step(9)
+        for n in abi.FIELD_NAMES:
+            np.testing.assert_array_equal(h.download(n), want[n])
+    other = make_case(case, abi.MP_FP64)
+    with runtime.Simulation(other) as h:
+        with pytest.raises(runtime.MPulseError):
+            h.load_state(snap)

@@ -139,6 +139,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def follow_trace(sim, axis, z_start: int, steps: int = 16) -> list:
+    """FollowMax::calculate (followmax.cpp:73-113) of Ex along z through the
+    column `axis`, after each of `steps` steps (mp_follow_max)."""
+    ip, out = z_start, []
+    for _ in range(steps):
+        sim.step(1)
+        ip, x = sim.follow_max("Ex", 2, (axis[0], axis[1], ip), ip)
+        out.append(x)
+    return out
+
+
 def time_steps(sim, torch, steps: int, stream) -> tuple[float, int]:
     """Device time (s) of `steps` steps with CUDA events on the sim's stream."""
     L0 = sim.launches
@@ -198,6 +209,10 @@ def run_ours(args) -> dict:
     value = world * cells * args.steps / t_max / 1e9
     # FP32 state after warmup + steps, compared below with the FP64 form
     fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
+    # FollowMax of Ex along z through the beam axis, over the next steps
+    axis = (cfg.nx // 2, cfg.ny // 2)
+    z_start = int(np.argmax(np.abs(fp32_state["Ex"][1:-1, axis[1] - 1, axis[0] - 1]))) + 1
+    trace32 = follow_trace(sim, axis, z_start)
 
     # per-kernel device times (CUDA events around each launch, further steps)
     kt = sim.kernel_times(max(3, min(args.steps, 10)))
@@ -229,6 +244,7 @@ def run_ours(args) -> dict:
     sim64.step(args.warmup)
     dt64, _ = time_steps(sim64, torch, args.steps, stream)
     fp64_state = {n: sim64.download(n) for n in ("Ex", "Ey", "Ez")}
+    trace64 = follow_trace(sim64, axis, z_start)
     sim64.close()
     num = sum(float(np.sum((fp32_state[n] - fp64_state[n]) ** 2)) for n in fp32_state)
     den = sum(float(np.sum(fp64_state[n] ** 2)) for n in fp64_state)
@@ -250,6 +266,9 @@ def run_ours(args) -> dict:
         "fp64": {"value": round(value64, 4), "unit": UNIT, "ms_per_step": round(dt64 / args.steps * 1e3, 4)},
         "fp32_over_fp64": round(value / value64, 3) if value64 > 0 else None,
         "rel_l2_fp32_vs_fp64": rel,
+        "followmax": {"field": "Ex", "dim": "z", "line_xy": list(axis), "steps": len(trace32),
+                      "fp32": [round(x, 4) for x in trace32], "fp64": [round(x, 4) for x in trace64],
+                      "max_abs_diff": float(np.max(np.abs(np.array(trace32) - np.array(trace64))))},
         "adjoint_forward_ratio": adjoint["fp32"]["ratio"] if adjoint else None,
         "adjoint": adjoint,
         "roofline": roofline, "step_roofline": step_roofline,

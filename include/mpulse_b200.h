@@ -334,6 +334,39 @@ long long mp_launch_count(mp_ctx *ctx);
 int mp_kernel_times(mp_ctx *ctx, int n_steps, double *e_half_ms, double *b_half_ms,
                     double *sources_ms);
 
+/* Field initialisers (FieldSimulation's "pulse_init", "gauss_init",
+ * "wave_init", src/fieldsim.cpp:157-168), evaluated on the device in FP64
+ * over the stored cells: the interior x / y columns of every z plane.  MPulse
+ * also writes the x / y ghost cells; here they are the periodic images. */
+typedef enum mp_init_kind {
+  MP_INIT_PULSE = 1,        /* GaussPulseInit::init, src/pulseinit.cpp:7-74:
+                               keys k (= k[2]), r0, z0, zc, C, Bx, By, bound */
+  MP_INIT_PLANE_GAUSS = 2,  /* PlaneGaussPulseInit::init, src/gaussinit.cpp:7-82:
+                               keys kx, ky, kz (whole numbers), Bx, By, Bz */
+  MP_INIT_WAVE = 3          /* PlaneWaveInit::init, src/waveinit.cpp:9-60 (adds to
+                               the fields): kx, ky, kz (whole numbers), Bx, By, Bz, eps */
+} mp_init_kind;
+
+typedef struct mp_init {
+  int kind;       /* mp_init_kind */
+  double k[3];    /* kx ky kz */
+  double B[3];    /* Bx By Bz */
+  double r0, z0, zc, C, eps;
+  int bound;      /* pulse_init: planes 0..bound-1 and nz+2-bound..nz+1 are left as they are */
+} mp_init;
+
+/* Fills *init with the MakeParamMap defaults of `kind` (pulseinit.cpp:77-89,
+ * gaussinit.cpp:85-95, waveinit.cpp:63-74). */
+void mp_init_defaults(int kind, mp_init *init);
+int mp_initialize(mp_ctx *ctx, const mp_init *init);
+
+/* FollowMax::calculate (src/followmax.cpp:73-113) on the device state: from
+ * the integer position *ipos along axis dim (0 x, 1 y, 2 z) of the line
+ * through MPulse cell pos[3], climb to a local maximum of the field (periodic
+ * wrap inside 1..n), return it in *ipos and the vertex of the parabola through
+ * it and its two neighbours in *position.  field: "Ex".."Bz". */
+int mp_follow_max(mp_ctx *ctx, const char *field, int dim, const int pos[3], int *ipos, double *position);
+
 /* Checkpoint / restart of the whole device state: the six fields, the PLRC
  * accumulators, the CPML psi of every face and the time (the injector state
  * is a function of the time).  The buffer is opaque, in the device precision,

@@ -130,6 +130,36 @@ class AdjointConfig(C.Structure):
     ]
 
 
+MP_INIT_PULSE, MP_INIT_PLANE_GAUSS, MP_INIT_WAVE = 1, 2, 3
+
+
+class Init(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("k", C.c_double * 3),
+        ("B", C.c_double * 3),
+        ("r0", C.c_double),
+        ("z0", C.c_double),
+        ("zc", C.c_double),
+        ("C", C.c_double),
+        ("eps", C.c_double),
+        ("bound", C.c_int),
+    ]
+
+
+def default_init(kind: int) -> Init:
+    """MakeParamMap defaults of pulse_init / gauss_init / wave_init
+    (pulseinit.cpp:77-89, gaussinit.cpp:85-95, waveinit.cpp:63-74)."""
+    q = Init()
+    q.kind = kind
+    q.k[:] = (1.0, 1.0, 1.0)
+    q.B[:] = (1.0, 1.0, 1.0)
+    q.r0 = q.z0 = q.zc = q.C = 1.0
+    q.eps = 1.0
+    q.bound = 0
+    return q
+
+
 def adjoint_config(kind: int, box, steps: int, checkpoint_every: int = 0, mem_budget: float = 0.0) -> AdjointConfig:
     a = AdjointConfig()
     a.kind = kind

@@ -100,7 +100,7 @@ struct mp_ctx {
   int *h_status = nullptr;
   double *staging = nullptr;
   double *d_diag = nullptr;   // diagnostics scratch: per-plane partials, then the result
-  double *h_diag = nullptr;   // pinned result
+  double *h_diag = nullptr;   // pinned results (two doubles)
   size_t staging_n = 0;
   long long time = 0;
   long long launches = 0;
@@ -661,7 +661,7 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_status), ST_COUNT * sizeof(int)), "status allocation");
   MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_status), ST_COUNT * sizeof(int)), "pinned allocation");
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_diag), size_t(g.nz + 3) * sizeof(double)), "diagnostics allocation");
-  MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_diag), sizeof(double)), "pinned allocation");
+  MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_diag), 2 * sizeof(double)), "pinned allocation");
 
   if (c->fp32) build_params<float>(c, c->epf, c->bpf, ikE_off, ikH_off, bzy_off, coef, numer, denom);
   else build_params<double>(c, c->epd, c->bpd, ikE_off, ikH_off, bzy_off, coef, numer, denom);
@@ -1791,6 +1791,128 @@ int mp_load_state(mp_ctx *c, const void *host, size_t bytes) {
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_err(c, e, "state copy");
   c->time = got.time;
+  return MP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// mp_initialize, mp_follow_max
+
+namespace mpb {
+template <typename T> cudaError_t launch_init(const InitParams &, void *const[6], cudaStream_t);
+template <typename T>
+cudaError_t launch_follow_max(const void *, int, int, int, long long, int, const int[3], int *, double *,
+                              cudaStream_t);
+}  // namespace mpb
+
+extern "C" {
+
+void mp_init_defaults(int kind, mp_init *q) {
+  if (!q) return;
+  memset(q, 0, sizeof(*q));
+  q->kind = kind;
+  for (int a = 0; a < 3; ++a) {
+    q->k[a] = 1.0;  // k / kx ky kz (pulseinit.cpp:79, gaussinit.cpp:87-89, waveinit.cpp:65-67)
+    q->B[a] = 1.0;  // Bx By Bz
+  }
+  q->r0 = q->z0 = q->zc = q->C = 1.0;  // pulseinit.cpp:80-83
+  q->eps = 1.0;                        // waveinit.cpp:71
+  q->bound = 0;                        // pulseinit.cpp:86
+}
+
+int mp_initialize(mp_ctx *c, const mp_init *q) {
+  if (!c || !q) return MP_ERR_INVALID;
+  const mp_config &g = c->cfg;
+  InitParams p;
+  memset(&p, 0, sizeof p);
+  p.kind = q->kind;
+  p.nx = g.nx; p.ny = g.ny; p.nz = g.nz;
+  p.plane = c->plane;
+  p.dx = g.dx; p.dy = g.dy; p.dz = g.dz;
+  // Globals::gridLow / gridHigh are 0 and n + 1 per axis (globals.cpp:44-45)
+  p.xh = 0.5 * double(g.nx + 1);
+  p.yh = 0.5 * double(g.ny + 1);
+  p.zh = 0.5 * double(g.nz + 1);
+  if (q->kind == MP_INIT_PULSE) {
+    // GaussPulseInit::init (pulseinit.cpp:7-31)
+    p.ex = q->B[1];
+    p.ey = -q->B[0];
+    p.bx = q->B[0];
+    p.by = q->B[1];
+    p.kz = q->k[2];
+    p.r0 = q->r0; p.z0 = q->z0; p.zc = q->zc; p.C = q->C;
+    p.k_lo = q->bound;
+    p.k_hi = g.nz + 1 - q->bound;
+  } else if (q->kind == MP_INIT_PLANE_GAUSS || q->kind == MP_INIT_WAVE) {
+    // PlaneGaussPulseInit::init (gaussinit.cpp:7-41), PlaneWaveInit::init (waveinit.cpp:9-36):
+    // kx, ky, kz are int parameters in MPulse
+    const int kx = int(q->k[0]), ky = int(q->k[1]), kz = int(q->k[2]);
+    const double bx = q->B[0], by = q->B[1], bz = q->B[2];
+    double ex = ky * bz - kz * by, ey = kz * bx - kx * bz, ez = kx * by - ky * bx;
+    const double bmag = std::sqrt(bx * bx + by * by + bz * bz);
+    const double factor = -bmag / std::sqrt(ex * ex + ey * ey + ez * ez);
+    if (q->kind == MP_INIT_PLANE_GAUSS) {
+      ex *= factor; ey *= factor; ez *= factor;
+      p.kx = kx / double(g.nx);
+      p.ky = ky / double(g.ny);
+      p.kz = kz / double(g.nz);
+      p.k_lo = 12;  // offsetz (gaussinit.cpp:42)
+      p.k_hi = g.nz + 1 - 12;
+    } else {
+      if (!(q->eps > 0)) return set_err(c, MP_ERR_INVALID, "wave_init: eps must be positive");
+      ex *= factor / std::sqrt(q->eps);
+      ey *= factor / std::sqrt(q->eps);
+      ez *= factor / std::sqrt(q->eps);
+      p.kx = 2 * M_PI * kx / double(g.nx);
+      p.ky = 2 * M_PI * ky / double(g.ny);
+      p.kz = 2 * M_PI * kz / double(g.nz);
+      p.k_lo = 0;
+      p.k_hi = g.nz + 1;
+    }
+    p.ex = ex; p.ey = ey; p.ez = ez;
+    p.bx = bx; p.by = by; p.bz = bz;
+  } else {
+    return set_err(c, MP_ERR_INVALID, "unknown initialiser kind %d", q->kind);
+  }
+  p.k_lo = std::max(p.k_lo, 0);
+  p.k_hi = std::min(p.k_hi, g.nz + 1);
+  cudaSetDevice(g.device);
+  cudaError_t e = c->fp32 ? launch_init<float>(p, c->F, c->stream) : launch_init<double>(p, c->F, c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "initialiser kernel");
+  c->launches++;
+  e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? MP_OK : cuda_err(c, e, "initialiser");
+}
+
+int mp_follow_max(mp_ctx *c, const char *field, int dim, const int pos[3], int *ipos, double *position) {
+  if (!c || !field || !pos || !ipos || !position) return MP_ERR_INVALID;
+  static const char *fn[6] = {"Ex", "Ey", "Ez", "Bx", "By", "Bz"};
+  int f = -1;
+  for (int q = 0; q < 6; ++q)
+    if (!strcmp(field, fn[q])) f = q;
+  if (f < 0) return set_err(c, MP_ERR_NAME, "follow_max: unknown field '%s'", field);
+  const mp_config &g = c->cfg;
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  if (dim < 0 || dim > 2) return set_err(c, MP_ERR_INVALID, "follow_max: dim must be 0, 1 or 2");
+  if (pos[0] < 1 || pos[0] > g.nx || pos[1] < 1 || pos[1] > g.ny || pos[2] < 0 || pos[2] > g.nz + 1)
+    return set_err(c, MP_ERR_INVALID, "follow_max: position outside the stored cells");
+  if (*ipos < 1 || *ipos > n3[dim]) return set_err(c, MP_ERR_INVALID, "follow_max: start index outside 1..%d", n3[dim]);
+  cudaSetDevice(g.device);
+  // the diagnostics scratch: the start index in, the result out
+  int *d_ip = reinterpret_cast<int *>(c->d_diag);
+  double *d_out = c->d_diag + 1;
+  cudaError_t e = cudaMemcpyAsync(d_ip, ipos, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = c->fp32 ? launch_follow_max<float>(c->F[f], g.nx, g.ny, g.nz, c->plane, dim, pos, d_ip, d_out, c->stream)
+                : launch_follow_max<double>(c->F[f], g.nx, g.ny, g.nz, c->plane, dim, pos, d_ip, d_out, c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "follow_max kernel");
+  c->launches++;
+  e = cudaMemcpyAsync(c->h_diag, c->d_diag, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "follow_max read");
+  memcpy(ipos, c->h_diag, sizeof(int));
+  *position = c->h_diag[1];
   return MP_OK;
 }
 

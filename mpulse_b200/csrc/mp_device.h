@@ -175,6 +175,18 @@ struct AdjParams {
   const T *obx, *oby;     // Bx, By of that state on the Sz plane (plane-sized)
 };
 
+// Field initialisers (mp_init_kernels.cu).
+struct InitParams {
+  int kind, nx, ny, nz;
+  long long plane;
+  double dx, dy, dz;
+  double ex, ey, ez, bx, by, bz;  // amplitudes after the reference's normalisation
+  double kx, ky, kz;              // pulse_init: kz; gauss_init / wave_init: the scaled nk*
+  double r0, z0, zc, C;
+  double xh, yh, zh;              // grid centre (MPulse index)
+  int k_lo, k_hi;                 // planes written
+};
+
 // Incident-source plane evaluation.
 struct SourceEvalParams {
   int kind;               // mp_source_kind

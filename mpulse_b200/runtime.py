@@ -26,7 +26,7 @@ EXPORTED = (
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
     "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_state_size", "mp_save_state",
-    "mp_load_state",
+    "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max",
 )
 
 _lib = None
@@ -95,6 +95,12 @@ def lib():
     L.mp_save_state.restype = C.c_int
     L.mp_load_state.argtypes = [vp, vp, sz]
     L.mp_load_state.restype = C.c_int
+    L.mp_init_defaults.argtypes = [C.c_int, C.POINTER(abi.Init)]
+    L.mp_init_defaults.restype = None
+    L.mp_initialize.argtypes = [vp, C.POINTER(abi.Init)]
+    L.mp_initialize.restype = C.c_int
+    L.mp_follow_max.argtypes = [vp, cp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), dp]
+    L.mp_follow_max.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
@@ -246,3 +252,17 @@ class Simulation:
     def load_state(self, data: bytes):
         buf = C.create_string_buffer(data, len(data))
         self._check(lib().mp_load_state(self._h, buf, len(data)))
+
+    # -- initialisers and FollowMax
+    def initialize(self, init: abi.Init):
+        """pulse_init / gauss_init / wave_init on the device (mp_initialize)."""
+        self._check(lib().mp_initialize(self._h, C.byref(init)))
+
+    def follow_max(self, field: str, dim: int, pos, ipos: int) -> tuple[int, float]:
+        """FollowMax::calculate from integer position ipos along dim through
+        MPulse cell pos: (new integer position, interpolated position)."""
+        p = (C.c_int * 3)(*pos)
+        ip = C.c_int(ipos)
+        out = C.c_double()
+        self._check(lib().mp_follow_max(self._h, field.encode(), dim, p, C.byref(ip), C.byref(out)))
+        return ip.value, out.value

@@ -1475,3 +1475,105 @@ void mpo_plrc_coefficients(const mpo_sim *s, double out[20]) {
   out[18] = s->sumChi0;
   out[19] = s->sumXi0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Field initialisers over the whole grid, ghost cells included, as MPulse
+ * writes them: GaussPulseInit::init (pulseinit.cpp:7-74),
+ * PlaneGaussPulseInit::init (gaussinit.cpp:7-82), PlaneWaveInit::init
+ * (waveinit.cpp:9-60). */
+int mpo_initialize(mpo_sim *s, const mp_init *q) {
+  const mp_config *c = &s->cfg;
+  double *Ex = s->F[0], *Ey = s->F[1], *Ez = s->F[2], *Bx = s->F[3], *By = s->F[4], *Bz = s->F[5];
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  /* Globals::gridLow / gridHigh: 0 and n + 1 per axis */
+  const double xh = 0.5 * (double)(c->nx + 1), yh = 0.5 * (double)(c->ny + 1), zh = 0.5 * (double)(c->nz + 1);
+  if (q->kind == MP_INIT_PULSE) {
+    const double ex = q->B[1], ey = -q->B[0], bx = q->B[0], by = q->B[1];
+    const double dx2 = c->dx * c->dx, dy2 = c->dy * c->dy;
+    const double nkz = c->dz * q->k[2];
+    const double rr0 = q->r0 * q->r0, zz0 = q->z0 * q->z0;
+    for (int i = 0; i < NX; ++i)
+      for (int j = 0; j < NY; ++j) {
+        const double iie = i - xh, jje = j - yh;
+        const double rre = (iie * iie * dx2 + jje * jje * dy2) / rr0;
+        const double iib = i + 0.5 - xh, jjb = j + 0.5 - yh;
+        const double rrb = (iib * iib * dx2 + jjb * jjb * dy2) / rr0;
+        for (int k = q->bound; k <= NZ - 1 - q->bound; ++k) {
+          const double nze = k * c->dz - q->zc, nzb = (k + 0.5) * c->dz - q->zc;
+          const double kze = k * nkz, kzb = (k + 0.5) * nkz;
+          const double ampe = cos(kze - q->C * rre) * exp(-nze * nze / zz0 - rre);
+          const double ampb = cos(kzb - q->C * rrb) * exp(-nzb * nzb / zz0 - rrb);
+          const size_t g = IDX(s, i, j, k);
+          Ex[g] = ex * ampe; Ey[g] = ey * ampe; Ez[g] = 0;
+          Bx[g] = bx * ampb; By[g] = by * ampb; Bz[g] = 0;
+        }
+      }
+    return MP_OK;
+  }
+  if (q->kind != MP_INIT_PLANE_GAUSS && q->kind != MP_INIT_WAVE) return MP_ERR_INVALID;
+  const int kx = (int)q->k[0], ky = (int)q->k[1], kz = (int)q->k[2];
+  const double bx = q->B[0], by = q->B[1], bz = q->B[2];
+  double ex = ky * bz - kz * by, ey = kz * bx - kx * bz, ez = kx * by - ky * bx;
+  const double bmag = sqrt(bx * bx + by * by + bz * bz);
+  const double factor = -bmag / sqrt(ex * ex + ey * ey + ez * ez);
+  if (q->kind == MP_INIT_PLANE_GAUSS) {
+    ex *= factor; ey *= factor; ez *= factor;
+    const double nkx = kx / (double)(c->nx), nky = ky / (double)(c->ny), nkz = kz / (double)(c->nz);
+    for (int i = 0; i < NX; ++i)
+      for (int j = 0; j < NY; ++j)
+        for (int k = 12; k <= NZ - 1 - 12; ++k) {
+          const double delta = 0.5;
+          const double pose = (i - xh) * nkx + (j - yh) * nky + (k - zh) * nkz;
+          const double posb = (i + delta - xh) * nkx + (j + delta - yh) * nky + (k + delta - zh) * nkz;
+          const double ampe = exp(-pose * pose), ampb = exp(-posb * posb);
+          const size_t g = IDX(s, i, j, k);
+          Ex[g] = ex * ampe; Ey[g] = ey * ampe; Ez[g] = ez * ampe;
+          Bx[g] = -bx * ampb; By[g] = -by * ampb; Bz[g] = -bz * ampb;
+        }
+    return MP_OK;
+  }
+  if (!(q->eps > 0)) return MP_ERR_INVALID;
+  ex *= factor / sqrt(q->eps); ey *= factor / sqrt(q->eps); ez *= factor / sqrt(q->eps);
+  const double nkx = 2 * M_PI * kx / (double)(c->nx), nky = 2 * M_PI * ky / (double)(c->ny),
+               nkz = 2 * M_PI * kz / (double)(c->nz);
+  for (int i = 0; i < NX; ++i)
+    for (int j = 0; j < NY; ++j)
+      for (int k = 0; k < NZ; ++k) {
+        const int ii = i - 1, jj = j - 1, kk = k - 1;
+        const size_t g = IDX(s, i, j, k);
+        Ex[g] += ex * cos((ii + 0.5) * nkx + jj * nky + kk * nkz);
+        Ey[g] += ey * cos(ii * nkx + (jj + 0.5) * nky + kk * nkz);
+        Ez[g] += ez * cos(ii * nkx + jj * nky + (kk + 0.5) * nkz);
+        Bx[g] += bx * cos(ii * nkx + (jj + 0.5) * nky + (kk + 0.5) * nkz);
+        By[g] += by * cos((ii + 0.5) * nkx + jj * nky + (kk + 0.5) * nkz);
+        Bz[g] += bz * cos((ii + 0.5) * nkx + (jj + 0.5) * nky + kk * nkz);
+      }
+  return MP_OK;
+}
+
+/* FollowMax::calculate (followmax.cpp:73-113) on the oracle grid: low = 0 and
+ * high = n + 1 along dim. */
+int mpo_follow_max(mpo_sim *s, const char *field, int dim, const int pos[3], int *ipos, double *position) {
+  const double *G = field_by_name(s, field);
+  if (!G || dim < 0 || dim > 2) return MP_ERR_INVALID;
+  const int n = dim == 0 ? s->cfg.nx : dim == 1 ? s->cfg.ny : s->cfg.nz;
+  const int low = 0, high = n + 1;
+  int p[3] = {pos[0], pos[1], pos[2]};
+  int ip = *ipos;
+  double mid, left, right;
+  int found;
+  do {
+    int pm = ip - 1, pp = ip + 1;
+    if (pm <= low) pm = high - 1;
+    if (pp >= high) pp = low + 1;
+    p[dim] = ip; mid = G[IDX(s, p[0], p[1], p[2])];
+    p[dim] = pm; left = G[IDX(s, p[0], p[1], p[2])];
+    p[dim] = pp; right = G[IDX(s, p[0], p[1], p[2])];
+    if (right > mid) { ip = pp; found = 0; }
+    else if (left > mid) { ip = pm; found = 0; }
+    else found = 1;
+  } while (!found);
+  *ipos = ip;
+  *position = ip + (left - right) / (2 * (left - 2 * mid + right));
+  return MP_OK;
+}

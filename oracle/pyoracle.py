@@ -63,6 +63,11 @@ def lib():
         L.mpo_cpml_layer.restype = C.c_int
         L.mpo_plrc_coefficients.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.mpo_plrc_coefficients.restype = None
+        L.mpo_initialize.argtypes = [C.c_void_p, C.POINTER(abi.Init)]
+        L.mpo_initialize.restype = C.c_int
+        L.mpo_follow_max.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double)]
+        L.mpo_follow_max.restype = C.c_int
         _lib = L
     return _lib
 
@@ -158,6 +163,20 @@ class OracleSim:
         z = lambda a: o[a:a + 6:2] + 1j * o[a + 1:a + 6:2]  # noqa: E731
         return {"dchi0": z(0), "dxi0": z(6), "crec": z(12), "sumChi0": o[18], "sumXi0": o[19]}
 
+    def initialize(self, init: abi.Init):
+        rc = lib().mpo_initialize(self.h, C.byref(init))
+        if rc != abi.MP_OK:
+            raise ValueError(f"mpo_initialize: {rc}")
+
+    def follow_max(self, field: str, dim: int, pos, ipos: int):
+        p = (C.c_int * 3)(*pos)
+        ip = C.c_int(ipos)
+        out = C.c_double()
+        rc = lib().mpo_follow_max(self.h, field.encode(), dim, p, C.byref(ip), C.byref(out))
+        if rc != abi.MP_OK:
+            raise ValueError(f"mpo_follow_max: {rc}")
+        return ip.value, out.value
+
     def source_field(self, src: int, which: int, i: int, j: int, l: int, time: int):
         out = np.zeros(3)
         rc = lib().mpo_source_field(self.h, src, which, i, j, l, time, _dptr(out))
@@ -191,8 +210,20 @@ def _fmt(x) -> str:
     return repr(float(x))
 
 
+def init_block(init: abi.Init) -> str:
+    """The setup-file block of a field initialiser (fieldsim.cpp:157-168)."""
+    if init.kind == abi.MP_INIT_PULSE:
+        return (f"pulse_init {{ k {_fmt(init.k[2])} r0 {_fmt(init.r0)} z0 {_fmt(init.z0)} zc {_fmt(init.zc)} "
+                f"C {_fmt(init.C)} Bx {_fmt(init.B[0])} By {_fmt(init.B[1])} bound {init.bound} }}")
+    ks = f"kx {int(init.k[0])} ky {int(init.k[1])} kz {int(init.k[2])}"
+    bs = f"Bx {_fmt(init.B[0])} By {_fmt(init.B[1])} Bz {_fmt(init.B[2])}"
+    if init.kind == abi.MP_INIT_PLANE_GAUSS:
+        return f"gauss_init {{ {ks} {bs} }}"
+    return f"wave_init {{ {ks} {bs} eps {_fmt(init.eps)} }}"
+
+
 def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver_name: str | None = None,
-               extra: str = "") -> str:
+               extra: str = "", inits: str = "") -> str:
     """MPulse setup file (rebuild.cpp grammar) describing `cfg`.  `solver_name`
     replaces the solver block's name (e.g. "fdtd-gpu-plrc-nonlin" for the B200
     plug-in, which reads the same keys); `extra` is appended to its body."""
@@ -242,6 +273,8 @@ def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver
     if extra:
         body.append(extra)
     init = f"raw_init {{ file {init_file} }}\n" if init_file else ""
+    if inits:
+        init += "  " + inits + "\n"
     return g + "fieldsim {\n  " + bnd + "\n  " + solver + " { " + " ".join(body) + " }\n  " + init + "}\n"
 
 
@@ -269,7 +302,7 @@ def full_to_plane(cfg: abi.Config, full: np.ndarray) -> np.ndarray:
 
 def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
                   names=abi.FIELD_NAMES, binary: str = REF_BIN, workdir: str | None = None,
-                  solver_name: str | None = None, extra: str = ""):
+                  solver_name: str | None = None, extra: str = "", inits: str = ""):
     """Runs the reference build for `steps` steps from the given initial fields
     (plane layout; missing components are zero) and returns
     ({name: plane-layout array}, timing dict).  With binary=REF_BIN_GPU and a
@@ -288,7 +321,7 @@ def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
                 f.write(np.ascontiguousarray(full).tobytes())
     setup = os.path.join(tmp, "setup.dat")
     with open(setup, "w") as f:
-        f.write(setup_text(cfg, steps, init_path, solver_name=solver_name, extra=extra))
+        f.write(setup_text(cfg, steps, init_path, solver_name=solver_name, extra=extra, inits=inits))
     r = subprocess.run([binary, setup, tmp, *names], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"reference failed ({r.returncode}): {r.stderr[-2000:]}")

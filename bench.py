@@ -353,6 +353,50 @@ def run_adjoint_profile(args) -> dict:
     return out
 
 
+def run_adjoint_large(args) -> dict:
+    """The large nonlinear adjoint workload (512 x 512 x 768, Sz objective,
+    FP32) for args.steps steps: forward (mp_objective) and mp_adjoint under a
+    memory budget of args.budget_gb GB for checkpoints and history (the
+    library picks the schedule); then the FP32 gradient against the FP64
+    adjoint on a 64^3 crop of the workload (16^3 design region, 320 steps)."""
+    from mpulse_b200 import runtime
+    out = {"adjoint_large_run": True, "steps": args.steps, "budget_gb": args.budget_gb}
+    cfg, des, adj = configs.c5_adjoint(abi.MP_FP32, steps=args.steps)
+    adj.mem_budget = args.budget_gb * 1e9
+    cells = cfg.nx * cfg.ny * cfg.nz
+
+    def fresh(c, d):
+        g = runtime.Simulation(c)
+        for k, v in d.items():
+            g.upload_design(k, v)
+        g.sync()
+        return g
+
+    with fresh(cfg, des) as g:
+        t0 = time.perf_counter()
+        out["J_forward"] = g.objective(adj)
+        out["forward_s"] = time.perf_counter() - t0
+    out["forward_gcells"] = cells * args.steps / out["forward_s"] / 1e9
+    with fresh(cfg, des) as g:
+        t0 = time.perf_counter()
+        out["J_adjoint"], gr = g.adjoint(adj)
+        out["adjoint_s"] = time.perf_counter() - t0
+    out["ratio"] = out["adjoint_s"] / out["forward_s"]
+    out["grad_norm_eps"] = float(np.linalg.norm(gr["DesignEps"]))
+    # 64^3 crop: FP32 against FP64
+    grads = {}
+    for prec in (abi.MP_FP32, abi.MP_FP64):
+        c2, d2, a2 = configs.c5_adjoint(prec, nx=64, ny=64, nz=64, steps=320, design=(16, 16, 16), design_z0=24,
+                                         sz_plane=52, src_d=6, cpml_d=6, medium_z0=10)
+        a2.mem_budget = 0
+        with fresh(c2, d2) as g:
+            _, grads[prec] = g.adjoint(a2)
+    out["crop_grad_rel_l2_fp32_vs_fp64"] = {
+        k: float(np.linalg.norm(grads[abi.MP_FP32][k] - grads[abi.MP_FP64][k]) / np.linalg.norm(grads[abi.MP_FP64][k]))
+        for k in ("DesignEps", "DesignChiScale")}
+    return out
+
+
 def run_profile(args) -> dict:
     """FP32 workload only: warm-up, then the timed steps; no other kernels."""
     import torch
@@ -508,12 +552,17 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only mp_objective + mp_adjoint of the adjoint workload for --steps steps (ncu captures)")
     ap.add_argument("--checkpoint", type=int, default=50, help="checkpoint interval of --adjoint-only")
+    ap.add_argument("--adjoint-large", action="store_true",
+                    help="the 512x512x768 nonlinear adjoint workload for --steps steps (minutes)")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="checkpoint budget of --adjoint-large")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.nz:
         WORKLOAD["nz"] = args.nz
-    if args.adjoint_only:
+    if args.adjoint_large:
+        out = run_adjoint_large(args)
+    elif args.adjoint_only:
         out = run_adjoint_profile(args)
     elif args.profile_only:
         out = run_profile(args)

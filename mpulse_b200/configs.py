@@ -239,3 +239,31 @@ def c4_adjoint(precision=abi.MP_FP64, n=96, seed=0) -> tuple:
     m = n // 2
     adj = abi.adjoint_config(abi.MP_OBJ_E2_BOX, (m - 3, m + 4, m - 3, m + 4, 77, 84), 1500, checkpoint_every=50)
     return c, {"DesignEps": eps.numpy()}, adj
+
+
+def c5_adjoint(precision=abi.MP_FP32, nx=512, ny=512, nz=768, steps=6000, seed=0, design=(128, 128, 64),
+               design_z0=320, sz_plane=700, src_d=20, cpml_d=16, medium_z0=64) -> tuple:
+    """Large nonlinear adjoint workload, 512 x 512 x 768 (dt = MEDIUM_COURANT
+    dx / c), 16-cell CPML on all faces, two-pole Lorentz medium with Kerr
+    chi3 E0^2 = 0.02 filling z >= 64, a design region of 128 x 128 x 64 cells
+    centred in x / y from z = 320 with eps_inf uniform in [1, 4] and a chi
+    factor uniform in [0.5, 1.5] (torch.Generator().manual_seed(seed)), a
+    focused pulse (waist 3 um at the design region's centre, lambda0 = 800 nm,
+    20 fs FWHM, the short-pulse closed form) injected at z = 20, and the
+    objective J = sum_t Sz dt dA through the plane z = 700; checkpoints within
+    a 120 GB budget.  Returns (config, {design map name: array}, adjoint config)."""
+    import torch
+
+    c = c3_plrc_kerr(precision, nx=nx, ny=ny, nz=nz, medium_z0=medium_z0, focus_z=design_z0 + design[2] // 2,
+                     src_d=src_d, chi=0.02)
+    c.cpml_d = cpml_d
+    c.cpml_sigma_max = sigma_max_for(1e-6, cpml_d, c.dz)
+    c.sources[0].waist = 3.0
+    bx, by, bz = design
+    x0, y0 = nx // 2 - bx // 2 + 1, ny // 2 - by // 2 + 1
+    c.design_box[:] = (x0, x0 + bx - 1, y0, y0 + by - 1, design_z0, design_z0 + bz - 1)
+    g = torch.Generator().manual_seed(seed)
+    eps = 1.0 + 3.0 * torch.rand((bz, by, bx), generator=g, dtype=torch.float64)
+    chi = 0.5 + torch.rand((bz, by, bx), generator=g, dtype=torch.float64)
+    adj = abi.adjoint_config(abi.MP_OBJ_SZ_PLANE, (1, nx, 1, ny, sz_plane, sz_plane), steps, mem_budget=120e9)
+    return c, {"DesignEps": eps.numpy(), "DesignChiScale": chi.numpy()}, adj

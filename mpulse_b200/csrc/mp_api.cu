@@ -15,6 +15,7 @@
 #include "mp_pulse_math.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>  // header-only NVTX: ranges for Nsight timelines, no cost without a tool
 
 #include <algorithm>
 #include <complex>
@@ -125,6 +126,12 @@ struct mp_ctx {
 };
 
 namespace {
+
+// An NVTX range over a scope (the host side of one phase).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 int set_err(mp_ctx *c, int code, const char *fmt, ...) {
   char buf[512];
@@ -802,6 +809,7 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
     int K = c->nsrc ? std::min(c->src_batch, n_steps - t) : n_steps - t;
     cudaError_t e;
     if (c->nsrc) {
+      NvtxRange nv("mp sources");
       if (tm) cudaEventRecord(tm->ev[4], c->stream);
       if (c->gauss) {
         // the block holding this step (computed here when it changes); the
@@ -840,6 +848,7 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
         const int rc = hooks->before(t + q);
         if (rc != MP_OK) return rc;
       }
+      NvtxRange nv("mp step");
       if (tm) cudaEventRecord(tm->ev[0], c->stream);
       e = c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
                  : launch_e_half<T>(ep, c->mode, c->np, c->stream);
@@ -1629,8 +1638,12 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     const cudaError_t err = copy_state(slot, true);
     return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint copy");
   };
-  ops.advance = [&](long long from, long long to) { return run(from, to, -1); };
+  ops.advance = [&](long long from, long long to) {
+    NvtxRange nv("mp_adjoint forward");
+    return run(from, to, -1);
+  };
   ops.leaf = [&](long long n0, long long n1) -> int {
+    NvtxRange nv("mp_adjoint chunk");
     cudaError_t err;
     if ((err = record(0, true)) != cudaSuccess) return cuda_err(c, err, "history copy");
     int r = run(n0, n1, n0);
@@ -1691,6 +1704,7 @@ int mp_objective(mp_ctx *c, const mp_adjoint_config *a, double *J) {
 int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_eps, double *grad_deps_scale,
                double *grad_chi_scale) {
   if (!c || !a || !J) return MP_ERR_INVALID;
+  NvtxRange nv("mp_adjoint");
   int rc = check_objective(c, a);
   if (rc != MP_OK) return rc;
   if (c->mode != MODE_PLRC_LIN && c->mode != MODE_PLRC_NONLIN)

@@ -1431,19 +1431,25 @@ long long schedule_steps(long long Tn, long long Kh, int slots) {
   return steps;
 }
 
-// History chunk Kh and checkpoint slots for Tn steps: checkpoint_every K > 0
-// gives chunks of K with a checkpoint at every chunk start; a memory budget
-// (bytes for (slots + 1) states and Kh + 1 steps of history) gives the plan
-// with the fewest forward steps; neither keeps the whole history.
-bool plan_schedule(long long Tn, long long every, double budget, size_t S, size_t H, long long *Kh, int *slots) {
+// History chunk Kh, checkpoint slots and history buffers for Tn steps:
+// checkpoint_every K > 0 gives chunks of K with a checkpoint at every chunk
+// start; a memory budget (bytes for (slots + 1) states and Kh + 1 steps of
+// history per buffer) gives the plan with the fewest forward steps; neither
+// keeps the whole history.  A second history buffer, which lets the forward
+// run of one chunk overlap the reverse pass of the last, is taken when there
+// are several chunks and (under a budget) it fits beside the chosen plan.
+bool plan_schedule(long long Tn, long long every, double budget, size_t S, size_t H, long long *Kh, int *slots,
+                   int *nbuf) {
   if (every > 0) {
     *Kh = std::min(every, Tn);
     *slots = int((Tn + *Kh - 1) / *Kh);
+    *nbuf = *Kh < Tn ? 2 : 1;
     return true;
   }
   if (!(budget > 0)) {
     *Kh = Tn;
     *slots = 1;
+    *nbuf = 1;
     return true;
   }
   long long best = -1;
@@ -1457,6 +1463,7 @@ bool plan_schedule(long long Tn, long long every, double budget, size_t S, size_
       best = cost;
       *Kh = kh;
       *slots = s;
+      *nbuf = m > 1 && room - double(s) * double(S) >= double(kh + 1) * double(H) ? 2 : 1;
     }
   }
   return best >= 0;
@@ -1480,7 +1487,8 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   const size_t H = 3 * fbytes + (sz ? 2 * pbytes : 0);
   long long Kh = 0;  // steps per history chunk
   int slots = 0;     // state checkpoints (the initial state included)
-  if (!plan_schedule(Tn, a->checkpoint_every, a->mem_budget, S, H, &Kh, &slots))
+  int nbuf = 1;      // history buffers
+  if (!plan_schedule(Tn, a->checkpoint_every, a->mem_budget, S, H, &Kh, &slots, &nbuf))
     return set_err(c, MP_ERR_NO_MEMORY,
                    "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
                    a->mem_budget, S, H);
@@ -1488,12 +1496,41 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
 
   DevBufs buf(c->stream);
   cudaError_t e;
-  char *ckpt, *hist;
+  char *ckpt, *hist[2] = {nullptr, nullptr};
   double *terms;
   if ((e = buf.alloc(reinterpret_cast<void **>(&ckpt), size_t(slots + 1) * S)) != cudaSuccess ||
-      (e = buf.alloc(reinterpret_cast<void **>(&hist), size_t(K + 1) * H)) != cudaSuccess ||
+      (e = buf.alloc(reinterpret_cast<void **>(&hist[0]), size_t(K + 1) * H)) != cudaSuccess ||
       (e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(Tn) + 1) * sizeof(double))) != cudaSuccess)
     return cuda_err(c, e, "checkpoint allocation");
+  if (nbuf == 2 && buf.alloc(reinterpret_cast<void **>(&hist[1]), size_t(K + 1) * H) != cudaSuccess) {
+    cudaGetLastError();  // no room for the second buffer: chunks run forward and back in turn
+    nbuf = 1;
+  }
+  // The reverse pass runs on a second stream: the adjoint kernels of one chunk
+  // overlap the forward run of the next, which only shares the history buffer
+  // the chunk reads (events order the two).
+  struct RevStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fwd[2] = {nullptr, nullptr}, rev[2] = {nullptr, nullptr};
+    bool used[2] = {false, false};
+    ~RevStream() {
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+      for (int q = 0; q < 2; ++q) {
+        if (fwd[q]) cudaEventDestroy(fwd[q]);
+        if (rev[q]) cudaEventDestroy(rev[q]);
+      }
+    }
+  } rs;
+  if ((e = cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_err(c, e, "cudaStreamCreate");
+  for (int q = 0; q < 2; ++q)
+    if ((e = cudaEventCreateWithFlags(&rs.fwd[q], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&rs.rev[q], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_err(c, e, "cudaEventCreate");
+  int cur = 0;  // history buffer of the chunk being run forward
   AdjParams<T> p = AdjParams<T>();
   for (int q = 0; q < 3; ++q) {
     void *eb, *bb, *gg;
@@ -1578,7 +1615,7 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   // E of a state into a history slot (copied, or, via ep.hist, stored by the E
   // kernel of the step that produces it); Bx, By on the Sz plane are copied
   auto record = [&](long long slot, bool withE) -> cudaError_t {
-    char *h = hist + size_t(slot) * H;
+    char *h = hist[cur] + size_t(slot) * H;
     for (int q = 0; q < 3 && withE; ++q) {
       cudaError_t err = cudaMemcpyAsync(h + q * fbytes, c->F[q], fbytes, cudaMemcpyDeviceToDevice, c->stream);
       if (err != cudaSuccess) return err;
@@ -1592,10 +1629,10 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     return cudaSuccess;
   };
   auto slot_e = [&](long long slot, int q) {
-    return reinterpret_cast<const T *>(hist + size_t(slot) * H + q * fbytes);
+    return reinterpret_cast<const T *>(hist[cur] + size_t(slot) * H + q * fbytes);
   };
   auto slot_b = [&](long long slot, int q) {
-    return sz ? reinterpret_cast<const T *>(hist + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
+    return sz ? reinterpret_cast<const T *>(hist[cur] + size_t(slot) * H + 3 * fbytes + q * pbytes) : nullptr;
   };
   auto hist_into = [&](long long slot) {
     for (int q = 0; q < 3; ++q) ep.hist[q] = slot < 0 ? nullptr : const_cast<T *>(slot_e(slot, q));
@@ -1645,18 +1682,28 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   ops.leaf = [&](long long n0, long long n1) -> int {
     NvtxRange nv("mp_adjoint chunk");
     cudaError_t err;
+    // the buffer is free once the reverse pass of the chunk that used it is done
+    if (rs.used[cur] && (err = cudaStreamWaitEvent(c->stream, rs.rev[cur], 0)) != cudaSuccess)
+      return cuda_err(c, err, "cudaStreamWaitEvent");
     if ((err = record(0, true)) != cudaSuccess) return cuda_err(c, err, "history copy");
     int r = run(n0, n1, n0);
     if (r != MP_OK) return r;
-    if (n1 == Tn && !at_end) {
-      // the first time the run reaches the end: J, the final state, the start of the adjoint
+    const bool first = n1 == Tn && !at_end;
+    if (first) {
+      // the first time the run reaches the end: J, the final state
       at_end = true;
       if ((err = copy_state(slots, true)) != cudaSuccess) return cuda_err(c, err, "checkpoint copy");
       if ((r = read_sum(c, terms, Tn, J)) != MP_OK || (r = mp_check_status(c)) != MP_OK) return r;
+    }
+    if ((err = cudaEventRecord(rs.fwd[cur], c->stream)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(rs.s, rs.fwd[cur], 0)) != cudaSuccess)
+      return cuda_err(c, err, "event");
+    if (first) {
+      // the start of the adjoint
       for (int q = 0; q < 3; ++q) p.En[q] = slot_e(n1 - n0, q);
       p.obx = slot_b(n1 - n0, 0);
       p.oby = slot_b(n1 - n0, 1);
-      if ((err = launch_adj_init<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint init kernel");
+      if ((err = launch_adj_init<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint init kernel");
       c->launches++;
     }
     for (long long n = n1 - 1; n >= n0; --n) {
@@ -1667,10 +1714,13 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       p.obx = slot_b(n - n0, 0);
       p.oby = slot_b(n - n0, 1);
       p.add_obj = n >= 1;
-      if ((err = launch_adj_e<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint E kernel");
-      if ((err = launch_adj_b<T>(p, c->stream)) != cudaSuccess) return cuda_err(c, err, "adjoint B kernel");
+      if ((err = launch_adj_e<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint E kernel");
+      if ((err = launch_adj_b<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint B kernel");
       c->launches += 2;
     }
+    if ((err = cudaEventRecord(rs.rev[cur], rs.s)) != cudaSuccess) return cuda_err(c, err, "event");
+    rs.used[cur] = true;
+    cur = (cur + 1) % nbuf;
     return MP_OK;
   };
   if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
@@ -1679,6 +1729,7 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   long long live = 0;
   int rc = revolve(0, Tn, 0, free_slots, K, ops, live);
   if (rc != MP_OK) return rc;
+  if ((e = cudaStreamSynchronize(rs.s)) != cudaSuccess) return cuda_err(c, e, "adjoint");
   if ((e = copy_state(slots, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
   c->time = t0 + Tn;
   for (int q = 0; q < 3; ++q)

@@ -45,7 +45,8 @@ def _newer(target: str, deps) -> bool:
 
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+               glob.glob(os.path.join(INCLUDE, "*.h")))
     objs = []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")

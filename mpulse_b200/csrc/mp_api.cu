@@ -56,11 +56,19 @@ using namespace mpb;
 
 namespace {
 
-const int kFaceOrderAll[6] = {FACE_NORTH, FACE_SOUTH, FACE_EAST, FACE_WEST, FACE_UP, FACE_DOWN};
+constexpr int kFaceOrderAll[6] = {FACE_NORTH, FACE_SOUTH, FACE_EAST, FACE_WEST, FACE_UP, FACE_DOWN};
 const int kFaceOrderZ[2] = {FACE_UP, FACE_DOWN};
 thread_local char g_create_err[512];
 
-int face_dim(int f) { return (f == FACE_EAST || f == FACE_WEST) ? 0 : (f == FACE_NORTH || f == FACE_SOUTH) ? 1 : 2; }
+constexpr int face_dim(int f) {
+  return (f == FACE_EAST || f == FACE_WEST) ? 0 : (f == FACE_NORTH || f == FACE_SOUTH) ? 1 : 2;
+}
+// slot q of the kernels' face arrays holds kFaceOrderAll[q], whose axis the
+// kernels take as y, y, x, x, z, z
+static_assert(face_dim(kFaceOrderAll[0]) == 1 && face_dim(kFaceOrderAll[1]) == 1 &&
+                  face_dim(kFaceOrderAll[2]) == 0 && face_dim(kFaceOrderAll[3]) == 0 &&
+                  face_dim(kFaceOrderAll[4]) == 2 && face_dim(kFaceOrderAll[5]) == 2,
+              "face slots");
 bool face_low(int f) { return f == FACE_WEST || f == FACE_SOUTH || f == FACE_DOWN; }
 
 struct LayerHost {
@@ -511,8 +519,10 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
       const int f = order[q];
       const int dim = face_dim(f);
       const int n = n3[dim];
+      // the kernels find a face's axis from its slot: the order of kFaceOrderAll
+      const int slot = g.cpml == MP_CPML_ALL ? q : q + 4;
       for (int isH = 0; isH < 2; ++isH) {
-        LayerHost &L = isH ? c->cpH[q] : c->cpE[q];
+        LayerHost &L = isH ? c->cpH[slot] : c->cpE[slot];
         // the reference layer along dim (getBorderExtent with the distances of
         // cpml_border.cpp:353 and :441-450)
         const int distance = (isH && face_low(f)) ? 0 : 1;

@@ -29,6 +29,32 @@ __device__ __forceinline__ bool finite3(double a, double b, double c) {
   return isfinite(a) && isfinite(b) && isfinite(c);
 }
 
+// CPML faces sit in fixed slots of EParams::cpml / BParams::cpml, in MPulse's
+// current order (north, south, east, west, up, down): slots 0-1 are y faces,
+// 2-3 x faces, 4-5 z faces.  With the slot known at compile time the axis of
+// every face is too.
+__host__ __device__ constexpr int face_axis(int f) { return f < 2 ? 1 : (f < 4 ? 0 : 2); }
+
+// Bit f (f < 4) set when the x / y face in slot f contains column (i, j):
+// computed once per thread, outside the z-march.
+template <typename T>
+__device__ __forceinline__ unsigned face_column_mask(const CpmlFace<T> (&cpml)[6], int i, int j) {
+  unsigned m = 0;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const int idx = face_axis(f) == 0 ? i + 1 : j + 1;
+    if (cpml[f].active && idx >= cpml[f].lo && idx <= cpml[f].hi) m |= 1u << f;
+  }
+  return m;
+}
+
+// True when plane k lies in one of the z faces (slots 4, 5).
+template <typename T>
+__device__ __forceinline__ bool z_face_plane(const CpmlFace<T> (&cpml)[6], int k) {
+  return (cpml[4].active && k >= cpml[4].lo && k <= cpml[4].hi) ||
+         (cpml[5].active && k >= cpml[5].lo && k <= cpml[5].hi);
+}
+
 // Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
 // (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped.
 __device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
@@ -127,9 +153,9 @@ __device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int
   }
 }
 
-template <typename T, int MODE, int NP, bool DESIGN = false>
+template <typename T, int MODE, int NP, bool DESIGN = false, bool FACES = true>
 __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
-                                       const EIn<T> &v, T ikx, T iky, T ikz,
+                                       unsigned cmask, const EIn<T> &v, T ikx, T iky, T ikz,
                                        typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
                                        T &ezn) {
   const T dt = p.dt;
@@ -143,11 +169,12 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const CpmlFace<T> &F = p.cpml[f];
-    const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
-    cin[f] = (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) && F.active && idx >= F.lo && idx <= F.hi;
+    const int idx = face_axis(f) == 0 ? i + 1 : face_axis(f) == 1 ? j + 1 : k;
+    cin[f] = FACES && (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) &&
+             (f < 4 ? ((cmask >> f) & 1u) != 0 : (F.active && k >= F.lo && k <= F.hi));
     if (cin[f]) {
-      if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
-      else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+      if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+      else if (face_axis(f) == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
       else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
       cp0[f] = F.psi0[cli[f]];
       cp1[f] = F.psi1[cli[f]];
@@ -172,7 +199,7 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;
-    const int dim = p.cpml[f].dim;
+    const int dim = face_axis(f);
     T d0, d1;  // differences of B along dim for psi0, psi1
     if (dim == 2) { d0 = -(v.by - v.by_km); d1 = v.bx - v.bx_km; }
     else if (dim == 0) { d0 = -(v.bz - v.bz_xm); d1 = v.by - v.by_xm; }
@@ -274,9 +301,9 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 // One cell of the B half: CPML psi_H (cpml_border.cpp:499-527), the magnetic
 // current sum and plrcStepB (fdtd_plrc.cpp:263-293) / FDTD_Plain::stepB.
 // Returns the new B in bxn, byn, bzn.
-template <typename T>
-__device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k, long long col, const BIn<T> &v,
-                                       T ikx, T iky, T iky_bz, T ikz, T &bxn, T &byn, T &bzn) {
+template <typename T, bool FACES = true>
+__device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k, long long col, unsigned cmask,
+                                       const BIn<T> &v, T ikx, T iky, T iky_bz, T ikz, T &bxn, T &byn, T &bzn) {
   const T dt = p.dt;
   T cp0[6], cp1[6], cb[6], cc[6];
   int cli[6];
@@ -284,11 +311,11 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const CpmlFace<T> &F = p.cpml[f];
-    const int idx = F.dim == 0 ? i + 1 : F.dim == 1 ? j + 1 : k;
-    cin[f] = F.active && idx >= F.lo && idx <= F.hi;
+    const int idx = face_axis(f) == 0 ? i + 1 : face_axis(f) == 1 ? j + 1 : k;
+    cin[f] = FACES && (f < 4 ? ((cmask >> f) & 1u) != 0 : (F.active && k >= F.lo && k <= F.hi));
     if (cin[f]) {
-      if (F.dim == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
-      else if (F.dim == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
+      if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
+      else if (face_axis(f) == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
       else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
       cp0[f] = F.psi0[cli[f]];
       cp1[f] = F.psi1[cli[f]];
@@ -311,7 +338,7 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;
-    const int dim = p.cpml[f].dim;
+    const int dim = face_axis(f);
     T d0, d1;
     if (dim == 2) { d0 = v.ey_kp - v.ey; d1 = -(v.ex_kp - v.ex); }
     else if (dim == 0) { d0 = v.ez_xp - v.ez; d1 = -(v.ey_xp - v.ey); }

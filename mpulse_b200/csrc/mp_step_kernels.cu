@@ -64,6 +64,10 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
   T *__restrict__ Ez = p.E[2];
   const T ikx = ld(p.ik[0] + i + 1);
   const T iky = ld(p.ik[1] + j + 1);
+  // CPML faces: the x / y faces of this warp's columns are fixed through the
+  // z-march; warps with none skip the face code on planes outside the z faces
+  const unsigned cmask = face_column_mask(p.cpml, i, j);
+  const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
 
   int km = k0 - 1;
   if (p.zperiodic && km == 0) km = p.nz;
@@ -97,7 +101,10 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
         for (int c = 0; c < 3; ++c) q[n][c] = reinterpret_cast<const T2 *>(p.psi[n][c])[pi];
     }
     T exn, eyn, ezn;
-    e_cell<T, MODE, NP, DESIGN>(p, i, j, k, col, med, v, ikx, iky, ikz, q, exn, eyn, ezn);
+    if (warp_xy || z_face_plane(p.cpml, k))
+      e_cell<T, MODE, NP, DESIGN, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
+    else
+      e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
     // ---- stores
     Ex[base + col] = exn;
     Ey[base + col] = eyn;
@@ -142,6 +149,8 @@ __global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BPa
   const T ikx = ld(p.ik[0] + i + 1);
   const T iky = ld(p.ik[1] + j + 1);
   const T iky_bz = ld(p.ik_bz_y + j + 1);
+  const unsigned cmask = face_column_mask(p.cpml, i, j);
+  const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
 
   // loads of plane k (ex, ey of plane k are carried from the previous plane)
   auto load = [&](int k, T ex_k, T ey_k, BIn<T> &v) {
@@ -175,7 +184,10 @@ __global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BPa
 #endif
     const T ikz = ld(p.ik[2] + k);
     T bxn, byn, bzn;
-    b_cell<T>(p, i, j, k, col, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
+    if (warp_xy || z_face_plane(p.cpml, k))
+      b_cell<T, true>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
+    else
+      b_cell<T, false>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
     Bx[base + col] = bxn;
     By[base + col] = byn;
     Bz[base + col] = bzn;

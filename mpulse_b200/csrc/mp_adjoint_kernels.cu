@@ -27,19 +27,24 @@
 
 #include <cuda_runtime.h>
 
-// Resident blocks per SM asked of the register allocator, per precision.
+// Blocks of 32 x MPB_ADJ_BLOCK_Y columns; resident threads per SM asked of
+// the register allocator, per precision.
+#ifndef MPB_ADJ_BLOCK_Y
+#define MPB_ADJ_BLOCK_Y 4
+#endif
 #ifndef MPB_ADJ_E_MIN_F
-#define MPB_ADJ_E_MIN_F 2
+#define MPB_ADJ_E_MIN_F 512
 #endif
 #ifndef MPB_ADJ_E_MIN_D
-#define MPB_ADJ_E_MIN_D 2
+#define MPB_ADJ_E_MIN_D 512
 #endif
 #ifndef MPB_ADJ_B_MIN_F
-#define MPB_ADJ_B_MIN_F 3
+#define MPB_ADJ_B_MIN_F 768
 #endif
 #ifndef MPB_ADJ_B_MIN_D
-#define MPB_ADJ_B_MIN_D 2
+#define MPB_ADJ_B_MIN_D 512
 #endif
+#define MPB_ADJ_THREADS (32 * MPB_ADJ_BLOCK_Y)
 
 namespace mpb {
 
@@ -90,7 +95,7 @@ __device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, long long l
 // the design gradients are FP64.  One thread per (x, y) column marches up a
 // chunk of planes, carrying the z-neighbours in registers.
 template <typename T, int NP>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_ADJ_E_MIN_D)
+__global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_ADJ_E_MIN_D) / MPB_ADJ_THREADS)
     adj_e_kernel(const AdjParams<T> p) {
   typedef T R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -351,7 +356,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_AD
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D)
+__global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D) / MPB_ADJ_THREADS)
     adj_b_kernel(const AdjParams<T> p) {
   typedef T R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,7 +566,8 @@ __global__ void __launch_bounds__(256) sum_terms_kernel(const double *terms, lon
 
 template <typename T>
 cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
-  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, (p.nz + p.kchunk_e - 1) / p.kchunk_e);
+  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
+      g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + p.kchunk_e - 1) / p.kchunk_e);
   switch (p.np) {
     case 0: adj_e_kernel<T, 0><<<g, b, 0, st>>>(p); break;
     case 1: adj_e_kernel<T, 1><<<g, b, 0, st>>>(p); break;
@@ -573,7 +579,8 @@ cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
 
 template <typename T>
 cudaError_t launch_adj_b(const AdjParams<T> &p, cudaStream_t st) {
-  const dim3 b(32, 8, 1), g((p.nx + 31) / 32, (p.ny + 7) / 8, (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b);
+  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
+      g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b);
   adj_b_kernel<T><<<g, b, 0, st>>>(p);
   return cudaGetLastError();
 }

@@ -55,6 +55,19 @@ __device__ __forceinline__ bool z_face_plane(const CpmlFace<T> (&cpml)[6], int k
          (cpml[5].active && k >= cpml[5].lo && k <= cpml[5].hi);
 }
 
+// The range of planes holding an injection plane (empty: lo > hi).
+template <typename P>
+__device__ __forceinline__ int2 source_plane_range(const P &p) {
+  int2 r = make_int2(1 << 30, -(1 << 30));
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+    if (s < p.n_src) {
+      r.x = min(r.x, p.src[s].plane);
+      r.y = max(r.y, p.src[s].plane);
+    }
+  return r;
+}
+
 // Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
 // (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped.
 __device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
@@ -153,7 +166,9 @@ __device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int
   }
 }
 
-template <typename T, int MODE, int NP, bool DESIGN = false, bool FACES = true>
+// SPECIAL = false: the caller guarantees that no CPML face contains the cell
+// and that k is no injection plane; the face and source code is left out.
+template <typename T, int MODE, int NP, bool DESIGN = false, bool SPECIAL = true>
 __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
                                        unsigned cmask, const EIn<T> &v, T ikx, T iky, T ikz,
                                        typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
@@ -170,7 +185,7 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
   for (int f = 0; f < 6; ++f) {
     const CpmlFace<T> &F = p.cpml[f];
     const int idx = face_axis(f) == 0 ? i + 1 : face_axis(f) == 1 ? j + 1 : k;
-    cin[f] = FACES && (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) &&
+    cin[f] = SPECIAL && (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) &&
              (f < 4 ? ((cmask >> f) & 1u) != 0 : (F.active && k >= F.lo && k <= F.hi));
     if (cin[f]) {
       if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
@@ -184,7 +199,7 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
   }
   T sa = T(0), sb = T(0);
   bool on_src = false;
-  if (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) {
+  if (SPECIAL && (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN)) {
     for (int s = 0; s < p.n_src; ++s) {
       if (k == p.src[s].plane) {
         sa = ld(p.src[s].v0 + col);
@@ -301,7 +316,7 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 // One cell of the B half: CPML psi_H (cpml_border.cpp:499-527), the magnetic
 // current sum and plrcStepB (fdtd_plrc.cpp:263-293) / FDTD_Plain::stepB.
 // Returns the new B in bxn, byn, bzn.
-template <typename T, bool FACES = true>
+template <typename T, bool SPECIAL = true>
 __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k, long long col, unsigned cmask,
                                        const BIn<T> &v, T ikx, T iky, T iky_bz, T ikz, T &bxn, T &byn, T &bzn) {
   const T dt = p.dt;
@@ -312,7 +327,7 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
   for (int f = 0; f < 6; ++f) {
     const CpmlFace<T> &F = p.cpml[f];
     const int idx = face_axis(f) == 0 ? i + 1 : face_axis(f) == 1 ? j + 1 : k;
-    cin[f] = FACES && (f < 4 ? ((cmask >> f) & 1u) != 0 : (F.active && k >= F.lo && k <= F.hi));
+    cin[f] = SPECIAL && (f < 4 ? ((cmask >> f) & 1u) != 0 : (F.active && k >= F.lo && k <= F.hi));
     if (cin[f]) {
       if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
       else if (face_axis(f) == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
@@ -325,7 +340,7 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
   }
   T sa = T(0), sb = T(0);
   bool on_src = false;
-  for (int s = 0; s < p.n_src; ++s) {
+  for (int s = 0; SPECIAL && s < p.n_src; ++s) {
     if (k == p.src[s].plane) {
       sa = ld(p.src[s].v0 + col);
       sb = ld(p.src[s].v1 + col);

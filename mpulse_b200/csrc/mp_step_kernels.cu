@@ -14,7 +14,7 @@
 //   (cpml_border.cpp:499-527), TF/SF M plane (incsource.t:112-145) and plrcStepB
 //   (fdtd_plrc.cpp:263-293).
 //
-// Thread mapping: one thread per (x, y) column, 32 x 8 columns per block; a
+// Thread mapping: one thread per (x, y) column, 32 x 4 columns per block; a
 // block marches up a chunk of z-planes so the z-neighbour of the previous plane
 // is carried in registers and every field element is read from HBM once per
 // half step (x/y neighbours are re-read through L1/L2).  The medium test, the
@@ -23,15 +23,24 @@
 // both kernels are HBM-bandwidth bound.
 #include "mp_cell.cuh"
 
-// Minimum resident blocks per SM asked of the register allocator.  Measured
-// on the 256x256x512 PLRC + Kerr workload (FP32): E half 1.083 ms with no
-// bound (114 registers), 0.917 ms with 3 blocks (80 registers, 28 B spilled),
-// 1.17 ms with 4 (64 registers, more spills); the B half does not move.
-#ifndef MPB_E_MIN_BLOCKS
-#define MPB_E_MIN_BLOCKS 3
+// Block shape 32 x BLOCK_Y columns (a warp is one row of 32 columns) and the
+// minimum resident threads per SM asked of the register allocator, 768 (80
+// registers).  Measured on the 256x256x512 PLRC + Kerr workload (FP32), with
+// 32 x 8 blocks: E half 1.083 ms with no bound (114 registers), 0.917 ms with
+// 768 threads (80 registers, 28 B spilled), 1.17 ms with 1024 (64 registers,
+// more spills); 32 x 4 blocks then took the E half from 0.872 to 0.859 ms and
+// the B half from 0.462 to 0.440 ms (32 x 2: no further gain).
+#ifndef MPB_E_BLOCK_Y
+#define MPB_E_BLOCK_Y 4
 #endif
-#ifndef MPB_B_MIN_BLOCKS
-#define MPB_B_MIN_BLOCKS 3
+#ifndef MPB_B_BLOCK_Y
+#define MPB_B_BLOCK_Y 4
+#endif
+#ifndef MPB_E_MIN_THREADS
+#define MPB_E_MIN_THREADS 768
+#endif
+#ifndef MPB_B_MIN_THREADS
+#define MPB_B_MIN_THREADS 768
 #endif
 // B half: issue the next plane's loads before the current plane's arithmetic.
 #ifndef MPB_B_PREFETCH
@@ -41,7 +50,8 @@
 namespace mpb {
 
 template <typename T, int MODE, int NP, bool DESIGN>
-__global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EParams<T> p) {
+__global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * MPB_E_BLOCK_Y))
+    e_half_kernel(const EParams<T> p) {
   typedef typename Vec2<T>::type T2;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based: MPulse i + 1
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -68,6 +78,7 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
   // z-march; warps with none skip the face code on planes outside the z faces
   const unsigned cmask = face_column_mask(p.cpml, i, j);
   const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
+  const int2 srck = source_plane_range(p);
 
   int km = k0 - 1;
   if (p.zperiodic && km == 0) km = p.nz;
@@ -101,7 +112,7 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
         for (int c = 0; c < 3; ++c) q[n][c] = reinterpret_cast<const T2 *>(p.psi[n][c])[pi];
     }
     T exn, eyn, ezn;
-    if (warp_xy || z_face_plane(p.cpml, k))
+    if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
       e_cell<T, MODE, NP, DESIGN, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
     else
       e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
@@ -126,7 +137,8 @@ __global__ void __launch_bounds__(256, MPB_E_MIN_BLOCKS) e_half_kernel(const EPa
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BParams<T> p) {
+__global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * MPB_B_BLOCK_Y))
+    b_half_kernel(const BParams<T> p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.nx || j >= p.ny) return;
@@ -151,6 +163,7 @@ __global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BPa
   const T iky_bz = ld(p.ik_bz_y + j + 1);
   const unsigned cmask = face_column_mask(p.cpml, i, j);
   const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
+  const int2 srck = source_plane_range(p);
 
   // loads of plane k (ex, ey of plane k are carried from the previous plane)
   auto load = [&](int k, T ex_k, T ey_k, BIn<T> &v) {
@@ -184,7 +197,7 @@ __global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BPa
 #endif
     const T ikz = ld(p.ik[2] + k);
     T bxn, byn, bzn;
-    if (warp_xy || z_face_plane(p.cpml, k))
+    if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
       b_cell<T, true>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
     else
       b_cell<T, false>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
@@ -202,14 +215,12 @@ __global__ void __launch_bounds__(256, MPB_B_MIN_BLOCKS) b_half_kernel(const BPa
 // ---------------------------------------------------------------------------
 // Launchers (called from mp_api.cu)
 
-static dim3 grid_for(int nx, int ny, int nk, int kchunk) {
-  return dim3((nx + 31) / 32, (ny + 7) / 8, (nk + kchunk - 1) / kchunk);
-}
 
 template <typename T, int MODE, bool DESIGN>
 static cudaError_t launch_e_np(const EParams<T> &p, int np, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
-  const dim3 g = grid_for(p.nx, p.ny, nk, p.kchunk), b(32, 8, 1);
+  const dim3 g((p.nx + 31) / 32, (p.ny + MPB_E_BLOCK_Y - 1) / MPB_E_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk),
+      b(32, MPB_E_BLOCK_Y, 1);
   switch (np) {
     case 0: e_half_kernel<T, MODE, 0, DESIGN><<<g, b, 0, st>>>(p); break;
     case 1: e_half_kernel<T, MODE, 1, DESIGN><<<g, b, 0, st>>>(p); break;
@@ -237,7 +248,8 @@ cudaError_t launch_e_half(const EParams<T> &p, int mode, int np, cudaStream_t st
 template <typename T>
 cudaError_t launch_b_half(const BParams<T> &p, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
-  b_half_kernel<T><<<grid_for(p.nx, p.ny, nk, p.kchunk), dim3(32, 8, 1), 0, st>>>(p);
+  const dim3 g((p.nx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk);
+  b_half_kernel<T><<<g, dim3(32, MPB_B_BLOCK_Y, 1), 0, st>>>(p);
   return cudaGetLastError();
 }
 

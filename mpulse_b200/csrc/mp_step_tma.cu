@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const T iky = ld(p.ik[1] + j + 1);
   const unsigned cmask = face_column_mask(p.cpml, i, j);
   const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
+  const int2 srck = source_plane_range(p);
   const bool wrap_x = (x0 == 0 && tx == 0);  // x-1 is the periodic image nx-1
   const bool wrap_y = (y0 == 0 && ty == 0);  // y-1 is the periodic image ny-1
   const long long colxm = (long long)j * p.nx + (p.nx - 1);
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     v.by_km = by_km;
     const T ikz = ld(p.ik[2] + k);
     T exn, eyn, ezn;
-    if (warp_xy || z_face_plane(p.cpml, k))
+    if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
       e_cell<T, MODE, NP, false, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
     else
       e_cell<T, MODE, NP, false, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
@@ -348,6 +349,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const T iky_bz = ld(p.ik_bz_y + j + 1);
   const unsigned cmask = face_column_mask(p.cpml, i, j);
   const bool warp_xy = __any_sync(__activemask(), cmask != 0u);
+  const int2 srck = source_plane_range(p);
   const bool wrap_x = (x0 + kTX == p.nx && tx == kTX - 1);  // x+1 is the image 0
   const bool wrap_y = (y0 + kTY == p.ny && ty == kTY - 1);  // y+1 is the image 0
   const long long colxp = (long long)j * p.nx;
@@ -401,7 +403,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     const T ikz = ld(p.ik[2] + k);
     T bxn, byn, bzn;
-    if (warp_xy || z_face_plane(p.cpml, k))
+    if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
       b_cell<T, true>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
     else
       b_cell<T, false>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);

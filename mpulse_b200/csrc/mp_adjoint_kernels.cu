@@ -59,12 +59,16 @@ __device__ __forceinline__ int face_pos(const AdjFace<T> &F, int idx) {
   return -1;
 }
 
-// Element of the x (D = 0) or y (D = 1) entry at plane k, axis position pos,
-// column (i, j).
+// Element of the x (D = 0) or y (D = 1) entry at axis position pos, column
+// (i, j) and plane k: face_col(..) + face_plane(.., k).  32-bit: the host
+// keeps every face array below 2^31 elements.
 template <int D, typename T>
-__device__ __forceinline__ long long face_xy_index(const AdjFace<T> &F, int pos, int i, int j, int k, int nx,
-                                                   int ny) {
-  return D == 0 ? ((long long)(k - F.zlo) * ny + j) * F.ex + pos : ((long long)(k - F.zlo) * F.ey + pos) * nx + i;
+__device__ __forceinline__ int face_col(const AdjFace<T> &F, int pos, int i, int j, int nx) {
+  return pos < 0 ? 0 : (D == 0 ? j * F.ex + pos : pos * nx + i);
+}
+template <int D, typename T>
+__device__ __forceinline__ int face_plane(const AdjFace<T> &F, int k, int nx, int ny) {
+  return D == 0 ? (k - F.zlo) * ny * F.ex : (k - F.zlo) * F.ey * nx;
 }
 
 // The components fed by psi0 / psi1 of a face along D (cpml_border.cpp:357-386):
@@ -80,7 +84,7 @@ __device__ __forceinline__ R comp1(const R v[3]) {
 
 // c * total at element li of an entry, or zero for pos < 0
 template <typename T, typename R>
-__device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, long long li, R c, R &w0, R &w1) {
+__device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, int li, R c, R &w0, R &w1) {
   if (pos >= 0) {
     w0 = c * R(F.a0[li]);
     w1 = c * R(F.a1[li]);
@@ -123,11 +127,21 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   const R hyco = hyo >= 0 ? R(HY.c[j + 1]) : R(0), hycm = hym >= 0 ? R(HY.c[jm + 1]) : R(0);
   const int exo = face_pos(EX, i + 1), eyo = face_pos(EY, j + 1);
   const R exb = exo >= 0 ? R(EX.b[i + 1]) : R(0), eyb = eyo >= 0 ? R(EY.b[j + 1]) : R(0);
+  const int plane = int(pl);
+  const int chxo = face_col<0>(HX, hxo, i, j, nx), chxm = face_col<0>(HX, hxm, im, j, nx);
+  const int chyo = face_col<1>(HY, hyo, i, j, nx), chym = face_col<1>(HY, hym, i, jm, nx);
+  const int cexo = face_col<0>(EX, exo, i, j, nx), ceyo = face_col<1>(EY, eyo, i, j, nx);
+  // warps whose columns lie in no x / y face skip the face code on planes
+  // outside the z faces
+  const bool warp_xy =
+      __any_sync(__activemask(), (hxo >= 0) || (hxm >= 0) || (hyo >= 0) || (hym >= 0) || (exo >= 0) || (eyo >= 0));
   // the z H face's c * total at plane k - 1, carried
   R cw0, cw1;
+  bool cw_on;
   {
     const int pz = face_pos(HZ, k0 - 1);
-    face_w(HZ, pz, (long long)pz * pl + col, pz >= 0 ? R(HZ.c[k0 - 1]) : R(0), cw0, cw1);
+    cw_on = pz >= 0;
+    face_w(HZ, pz, pz * plane + col, pz >= 0 ? R(HZ.c[k0 - 1]) : R(0), cw0, cw1);
   }
   const DesignParams &d = p.design;
   const bool dxy = i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1;
@@ -172,23 +186,27 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       u = d.chiscale[di];
     }
     // H-face totals (x, y at this column and x-1 / y-1; z at this plane) and
-    // E-face totals of this cell
-    R hx0o, hx1o, hx0m, hx1m, hy0o, hy1o, hy0m, hy1m, hz0, hz1;
-    const long long lhxo = face_xy_index<0>(HX, hxo, i, j, k, nx, ny), lhxm = face_xy_index<0>(HX, hxm, im, j, k, nx, ny);
-    const long long lhyo = face_xy_index<1>(HY, hyo, i, j, k, nx, ny), lhym = face_xy_index<1>(HY, hym, i, jm, k, nx, ny);
-    face_w(HX, hxo, lhxo, hxco, hx0o, hx1o);
-    face_w(HX, hxm, lhxm, hxcm, hx0m, hx1m);
-    face_w(HY, hyo, lhyo, hyco, hy0o, hy1o);
-    face_w(HY, hym, lhym, hycm, hy0m, hy1m);
-    const int hzp = face_pos(HZ, k);
-    face_w(HZ, hzp, (long long)hzp * pl + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1);
-    const long long lexo = face_xy_index<0>(EX, exo, i, j, k, nx, ny), leyo = face_xy_index<1>(EY, eyo, i, j, k, nx, ny);
-    const int ezp = face_pos(EZ, k);
-    const long long lezo = (long long)ezp * pl + col;
+    // E-face totals of this cell, on warps and planes that touch a face
+    const int hzp = face_pos(HZ, k), ezp = face_pos(EZ, k);
+    const bool fpl = warp_xy || cw_on || hzp >= 0 || ezp >= 0;
+    R hx0o = R(0), hx1o = R(0), hx0m = R(0), hx1m = R(0), hy0o = R(0), hy1o = R(0), hy0m = R(0), hy1m = R(0);
+    R hz0 = R(0), hz1 = R(0);
     R ex0 = R(0), ex1 = R(0), ey0 = R(0), ey1 = R(0), ez0 = R(0), ez1 = R(0), ezb = R(0);
-    if (exo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
-    if (eyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
-    if (ezp >= 0) { ez0 = EZ.a0[lezo]; ez1 = EZ.a1[lezo]; ezb = EZ.b[k]; }
+    int lexo = 0, leyo = 0, lezo = 0;
+    if (fpl) {
+      const int shx = face_plane<0>(HX, k, nx, ny), shy = face_plane<1>(HY, k, nx, ny);
+      face_w(HX, hxo, chxo + shx, hxco, hx0o, hx1o);
+      face_w(HX, hxm, chxm + shx, hxcm, hx0m, hx1m);
+      face_w(HY, hyo, chyo + shy, hyco, hy0o, hy1o);
+      face_w(HY, hym, chym + shy, hycm, hy0m, hy1m);
+      face_w(HZ, hzp, hzp * plane + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1);
+      lexo = cexo + face_plane<0>(EX, k, nx, ny);
+      leyo = ceyo + face_plane<1>(EY, k, nx, ny);
+      lezo = ezp * plane + col;
+      if (exo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
+      if (eyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
+      if (ezp >= 0) { ez0 = EZ.a0[lezo]; ez1 = EZ.a1[lezo]; ezb = EZ.b[k]; }
+    }
     R obx = R(0), oby = R(0);
     if (p.add_obj && oxy && p.obj_kind == 2 && k == p.oz0) {
       obx = p.obx[col];
@@ -207,14 +225,17 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     a[1] += dt * (-kxm * bz_xm + kxi * bz);
     // H faces: psi0 / psi1 feed (y, z) on x faces, (z, x) on y faces, (x, y) on
     // z faces; their differences of E run forward along the axis
-    a[2] += hx0m - hx0o;
-    a[1] += hx1o - hx1m;
-    a[0] += hy0m - hy0o;
-    a[2] += hy1o - hy1m;
-    a[1] += cw0 - hz0;
-    a[0] += hz1 - cw1;
+    if (fpl) {
+      a[2] += hx0m - hx0o;
+      a[1] += hx1o - hx1m;
+      a[0] += hy0m - hy0o;
+      a[2] += hy1o - hy1m;
+      a[1] += cw0 - hz0;
+      a[0] += hz1 - cw1;
+    }
     cw0 = hz0;
     cw1 = hz1;
+    cw_on = hzp >= 0;
 
     // ---- E half, locally
     R g[3], ne[3];
@@ -338,17 +359,19 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
         }
     }
     // E-face totals of this cell: b * total + dt * G
-    if (exo >= 0) {
-      EX.a0[lexo] = T(exb * ex0 + dt * comp0<0>(g));
-      EX.a1[lexo] = T(exb * ex1 + dt * comp1<0>(g));
-    }
-    if (eyo >= 0) {
-      EY.a0[leyo] = T(eyb * ey0 + dt * comp0<1>(g));
-      EY.a1[leyo] = T(eyb * ey1 + dt * comp1<1>(g));
-    }
-    if (ezp >= 0) {
-      EZ.a0[lezo] = T(ezb * ez0 + dt * comp0<2>(g));
-      EZ.a1[lezo] = T(ezb * ez1 + dt * comp1<2>(g));
+    if (fpl) {
+      if (exo >= 0) {
+        EX.a0[lexo] = T(exb * ex0 + dt * comp0<0>(g));
+        EX.a1[lexo] = T(exb * ex1 + dt * comp1<0>(g));
+      }
+      if (eyo >= 0) {
+        EY.a0[leyo] = T(eyb * ey0 + dt * comp0<1>(g));
+        EY.a1[leyo] = T(eyb * ey1 + dt * comp1<1>(g));
+      }
+      if (ezp >= 0) {
+        EZ.a0[lezo] = T(ezb * ez0 + dt * comp0<2>(g));
+        EZ.a1[lezo] = T(ezb * ez1 + dt * comp1<2>(g));
+      }
     }
     bx_km = bx;
     by_km = by;
@@ -384,12 +407,22 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
   const int hxo = face_pos(HX, i + 1), hyo = face_pos(HY, j + 1);
   const R hxb = hxo >= 0 ? R(HX.b[i + 1]) : R(0), hyb = hyo >= 0 ? R(HY.b[j + 1]) : R(0);
   const bool oxy = p.add_obj && p.obj_kind == 2 && i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
+  const int plane = int(pl);
+  const int cexo = face_col<0>(EX, exo, i, j, nx), cexp = face_col<0>(EX, exp_, ip, j, nx);
+  const int ceyo = face_col<1>(EY, eyo, i, j, nx), ceyp = face_col<1>(EY, eyp, i, jp, nx);
+  const int chxo = face_col<0>(HX, hxo, i, j, nx), chyo = face_col<1>(HY, hyo, i, j, nx);
+  // warps whose columns lie in no x / y face skip the face code on planes
+  // outside the z faces
+  const bool warp_xy =
+      __any_sync(__activemask(), (exo >= 0) || (exp_ >= 0) || (eyo >= 0) || (eyp >= 0) || (hxo >= 0) || (hyo >= 0));
   // G and the z E face's c * total at plane k, carried from the previous plane's k + 1
   R gx_k = gx[(long long)k0 * pl + col], gy_k = gy[(long long)k0 * pl + col];
   R zw0, zw1;
+  bool zw_on;
   {
     const int pz = face_pos(EZ, k0);
-    face_w(EZ, pz, (long long)pz * pl + col, pz >= 0 ? R(EZ.c[k0]) : R(0), zw0, zw1);
+    zw_on = pz >= 0;
+    face_w(EZ, pz, pz * plane + col, pz >= 0 ? R(EZ.c[k0]) : R(0), zw0, zw1);
   }
 
   for (int k = k0; k <= k1; ++k) {
@@ -401,24 +434,31 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     const R gx_yp = gx[base + colyp], gy_xp = gy[base + colxp], gz_xp = gz[base + colxp], gz_yp = gz[base + colyp];
     const R kzk = p.ikE[2][k], kzp = p.ikE[2][k + 1];
     R b[3] = {R(p.Bb[0][c0]), R(p.Bb[1][c0]), R(p.Bb[2][c0])};
-    // E faces: x / y hold planes 1..nz; z at plane k + 1 (plane k carried)
-    const bool ek = k >= 1;
-    R ex0o, ex1o, ex0p, ex1p, ey0o, ey1o, ey0p, ey1p, ez0p, ez1p;
-    face_w(EX, ek ? exo : -1, face_xy_index<0>(EX, exo, i, j, k, nx, ny), exco, ex0o, ex1o);
-    face_w(EX, ek ? exp_ : -1, face_xy_index<0>(EX, exp_, ip, j, k, nx, ny), excp, ex0p, ex1p);
-    face_w(EY, ek ? eyo : -1, face_xy_index<1>(EY, eyo, i, j, k, nx, ny), eyco, ey0o, ey1o);
-    face_w(EY, ek ? eyp : -1, face_xy_index<1>(EY, eyp, i, jp, k, nx, ny), eycp, ey0p, ey1p);
-    const int ezq = face_pos(EZ, k + 1);
-    face_w(EZ, ezq, (long long)ezq * pl + col, ezq >= 0 ? R(EZ.c[k + 1]) : R(0), ez0p, ez1p);
-    // H-face totals of this cell
+    // faces on warps and planes that touch one: E faces (x / y hold planes
+    // 1..nz; z at plane k + 1, plane k carried) and the H-face totals of this cell
+    const int ezq = face_pos(EZ, k + 1), hzp = face_pos(HZ, k);
+    const bool fpl = warp_xy || zw_on || ezq >= 0 || hzp >= 0;
+    R ex0o = R(0), ex1o = R(0), ex0p = R(0), ex1p = R(0), ey0o = R(0), ey1o = R(0), ey0p = R(0), ey1p = R(0);
+    R ez0p = R(0), ez1p = R(0);
     const bool hxk = hxo >= 0 && k >= HX.zlo, hyk = hyo >= 0 && k >= HY.zlo;
-    const long long lhx = face_xy_index<0>(HX, hxo, i, j, k, nx, ny), lhy = face_xy_index<1>(HY, hyo, i, j, k, nx, ny);
-    const int hzp = face_pos(HZ, k);
-    const long long lhz = (long long)hzp * pl + col;
+    int lhx = 0, lhy = 0, lhz = 0;
     R hx0 = R(0), hx1 = R(0), hy0 = R(0), hy1 = R(0), hz0 = R(0), hz1 = R(0), hzb = R(0);
-    if (hxk) { hx0 = HX.a0[lhx]; hx1 = HX.a1[lhx]; }
-    if (hyk) { hy0 = HY.a0[lhy]; hy1 = HY.a1[lhy]; }
-    if (hzp >= 0) { hz0 = HZ.a0[lhz]; hz1 = HZ.a1[lhz]; hzb = HZ.b[k]; }
+    if (fpl) {
+      if (k >= 1) {
+        const int sex = face_plane<0>(EX, k, nx, ny), sey = face_plane<1>(EY, k, nx, ny);
+        face_w(EX, exo, cexo + sex, exco, ex0o, ex1o);
+        face_w(EX, exp_, cexp + sex, excp, ex0p, ex1p);
+        face_w(EY, eyo, ceyo + sey, eyco, ey0o, ey1o);
+        face_w(EY, eyp, ceyp + sey, eycp, ey0p, ey1p);
+      }
+      face_w(EZ, ezq, ezq * plane + col, ezq >= 0 ? R(EZ.c[k + 1]) : R(0), ez0p, ez1p);
+      lhx = chxo + face_plane<0>(HX, k, nx, ny);
+      lhy = chyo + face_plane<1>(HY, k, nx, ny);
+      lhz = hzp * plane + col;
+      if (hxk) { hx0 = HX.a0[lhx]; hx1 = HX.a1[lhx]; }
+      if (hyk) { hy0 = HY.a0[lhy]; hy1 = HY.a1[lhy]; }
+      if (hzp >= 0) { hz0 = HZ.a0[lhz]; hz1 = HZ.a1[lhz]; hzb = HZ.b[k]; }
+    }
     const bool obj = oxy && k == p.oz0;
     R oex = R(0), oey = R(0);
     if (obj) {
@@ -438,14 +478,17 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     b[0] += dt * (-kyj * gzk + kyp * gz_yp);
     // E faces: psi0 / psi1 feed (y, z) on x faces, (z, x) on y faces, (x, y) on
     // z faces; their differences of B run backward along the axis
-    b[2] += -ex0o + ex0p;
-    b[1] += ex1o - ex1p;
-    b[0] += -ey0o + ey0p;
-    b[2] += ey1o - ey1p;
-    b[1] += -zw0 + ez0p;
-    b[0] += zw1 - ez1p;
+    if (fpl) {
+      b[2] += -ex0o + ex0p;
+      b[1] += ex1o - ex1p;
+      b[0] += -ey0o + ey0p;
+      b[2] += ey1o - ey1p;
+      b[1] += -zw0 + ez0p;
+      b[0] += zw1 - ez1p;
+    }
     zw0 = ez0p;
     zw1 = ez1p;
+    zw_on = ezq >= 0;
     // the objective's B term of the state before the step (Sz plane)
     if (obj) {
       b[0] -= R(p.obj_f) * oey;
@@ -455,17 +498,19 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     // ---- stores: B adjoint, H-face totals for the step before (b * total + dt * B adjoint)
 #pragma unroll
     for (int c = 0; c < 3; ++c) p.Bb[c][c0] = T(b[c]);
-    if (hxk) {
-      HX.a0[lhx] = T(hxb * hx0 + dt * comp0<0>(b));
-      HX.a1[lhx] = T(hxb * hx1 + dt * comp1<0>(b));
-    }
-    if (hyk) {
-      HY.a0[lhy] = T(hyb * hy0 + dt * comp0<1>(b));
-      HY.a1[lhy] = T(hyb * hy1 + dt * comp1<1>(b));
-    }
-    if (hzp >= 0) {
-      HZ.a0[lhz] = T(hzb * hz0 + dt * comp0<2>(b));
-      HZ.a1[lhz] = T(hzb * hz1 + dt * comp1<2>(b));
+    if (fpl) {
+      if (hxk) {
+        HX.a0[lhx] = T(hxb * hx0 + dt * comp0<0>(b));
+        HX.a1[lhx] = T(hxb * hx1 + dt * comp1<0>(b));
+      }
+      if (hyk) {
+        HY.a0[lhy] = T(hyb * hy0 + dt * comp0<1>(b));
+        HY.a1[lhy] = T(hyb * hy1 + dt * comp1<1>(b));
+      }
+      if (hzp >= 0) {
+        HZ.a0[lhz] = T(hzb * hz0 + dt * comp0<2>(b));
+        HZ.a1[lhz] = T(hzb * hz1 + dt * comp1<2>(b));
+      }
     }
     gx_k = gx_kp;
     gy_k = gy_kp;
@@ -500,12 +545,12 @@ __global__ void __launch_bounds__(256) adj_init_kernel(const AdjParams<T> p) {
   // H-face totals: dt times the adjoint of B
   const int hxo = face_pos(p.fh[0], i + 1), hyo = face_pos(p.fh[1], j + 1), hzo = face_pos(p.fh[2], k);
   if (hxo >= 0 && k >= p.fh[0].zlo) {
-    const long long li = face_xy_index<0>(p.fh[0], hxo, i, j, k, p.nx, p.ny);
+    const int li = face_col<0>(p.fh[0], hxo, i, j, p.nx) + face_plane<0>(p.fh[0], k, p.nx, p.ny);
     p.fh[0].a0[li] = T(p.dt * comp0<0>(b));
     p.fh[0].a1[li] = T(p.dt * comp1<0>(b));
   }
   if (hyo >= 0 && k >= p.fh[1].zlo) {
-    const long long li = face_xy_index<1>(p.fh[1], hyo, i, j, k, p.nx, p.ny);
+    const int li = face_col<1>(p.fh[1], hyo, i, j, p.nx) + face_plane<1>(p.fh[1], k, p.nx, p.ny);
     p.fh[1].a0[li] = T(p.dt * comp0<1>(b));
     p.fh[1].a1[li] = T(p.dt * comp1<1>(b));
   }

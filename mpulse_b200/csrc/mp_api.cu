@@ -1271,6 +1271,8 @@ int adj_faces(mp_ctx *c, DevBufs &buf, bool isH, const CpmlFace<T> *fw, AdjFace<
     F.ey = dim == 1 ? ntot : g.ny;
     const size_t zdepth = size_t(g.nz - F.zlo + 1);
     const size_t cells = dim == 2 ? size_t(ntot) * size_t(c->plane) : zdepth * size_t(F.ex) * size_t(F.ey);
+    if (cells >= (size_t(1) << 31))  // the adjoint kernels index face arrays in 32 bits
+      return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint: CPML face array of %zu cells exceeds 2^31", cells);
     void *a0, *a1;
     cudaError_t e;
     if ((e = buf.alloc(&a0, cells * sizeof(T))) != cudaSuccess || (e = buf.alloc(&a1, cells * sizeof(T))) != cudaSuccess)

@@ -43,6 +43,14 @@
 #define MPB_B_MIN_THREADS 768
 #endif
 // B half: issue the next plane's loads before the current plane's arithmetic.
+// B half: 16-byte loads along x where nx allows (its own occupancy: four
+// cells per thread need more registers).
+#ifndef MPB_B_VECTOR
+#define MPB_B_VECTOR 1
+#endif
+#ifndef MPB_BV_MIN_THREADS
+#define MPB_BV_MIN_THREADS 640
+#endif
 #ifndef MPB_B_PREFETCH
 #define MPB_B_PREFETCH 1
 #endif
@@ -212,6 +220,182 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
   }
 }
 
+// The B half with 16-byte loads along x: each thread owns V = 16 / sizeof(T)
+// consecutive cells of a row (nx a multiple of V), so a plane's loads are 8
+// vectors and two scalars (the x+1 neighbour of the last cell) per V cells,
+// and the z+1 plane of E is carried to the next plane.  Cells of warps or
+// planes with a CPML face or an injection plane go through b_cell one by one.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { typedef float4 type; };
+template <> struct Vec16<double> { typedef double2 type; };
+
+template <typename T>
+struct RowV {
+  T v[16 / sizeof(T)];
+};
+
+template <typename T>
+__device__ __forceinline__ RowV<T> ldv(const T *p) {
+  typedef typename Vec16<T>::type VT;
+  const VT x = __ldg(reinterpret_cast<const VT *>(p));
+  RowV<T> r;
+  memcpy(r.v, &x, sizeof(VT));
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ RowV<T> ldv_rw(const T *p) {
+  typedef typename Vec16<T>::type VT;
+  const VT x = *reinterpret_cast<const VT *>(p);
+  RowV<T> r;
+  memcpy(r.v, &x, sizeof(VT));
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void stv(T *p, const RowV<T> &r) {
+  typedef typename Vec16<T>::type VT;
+  VT x;
+  memcpy(&x, r.v, sizeof(VT));
+  *reinterpret_cast<VT *>(p) = x;
+}
+
+// psi_H of the face in slot F at one cell (cpml_border.cpp:499-527): updates
+// the layer arrays and adds the face's currents to m (MPulse's order: slots
+// in turn, as b_cell sums them).  d0 / d1: the differences of E along the
+// face's axis for psi0 / psi1.
+template <typename T, int F>
+__device__ __forceinline__ void b_face(const BParams<T> &p, int i, int j, int k, T d0, T d1, T (&m)[3]) {
+  constexpr int dim = face_axis(F);
+  const CpmlFace<T> &L = p.cpml[F];
+  const int idx = dim == 0 ? i + 1 : dim == 1 ? j + 1 : k;
+  int li;
+  if (dim == 2) li = ((k - L.lo) * p.ny + j) * p.nx + i;
+  else if (dim == 0) li = ((k - L.zlo) * p.ny + j) * L.ex + (i + 1 - L.lo);
+  else li = ((k - L.zlo) * L.ey + (j + 1 - L.lo)) * p.nx + i;
+  const T b = ld(L.b + idx), c = ld(L.c + idx);
+  const T c0 = b * L.psi0[li] + c * d0;
+  const T c1 = b * L.psi1[li] + c * d1;
+  L.psi0[li] = c0;
+  L.psi1[li] = c1;
+  if (dim == 2) { m[0] += c0; m[1] += c1; }
+  else if (dim == 0) { m[1] += c0; m[2] += c1; }
+  else { m[2] += c0; m[0] += c1; }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_BV_MIN_THREADS / (32 * MPB_B_BLOCK_Y))
+    b_half_vec_kernel(const BParams<T> p) {
+  constexpr int V = 16 / sizeof(T);
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i0 >= p.nx || j >= p.ny) return;
+  const int k0 = p.k_first + blockIdx.z * p.kchunk;
+  const int k1 = min(k0 + p.kchunk - 1, p.k_last);
+  if (k0 > k1) return;
+
+  const long long plane = p.plane;
+  const int jp = (j == p.ny - 1) ? 0 : j + 1;
+  const int il = (i0 + V == p.nx) ? 0 : i0 + V;  // x+1 of the last cell
+  const long long col = (long long)j * p.nx + i0;
+  const long long colyp = (long long)jp * p.nx + i0;
+  const long long colxl = (long long)j * p.nx + il;
+  const T *__restrict__ Ex = p.E[0];
+  const T *__restrict__ Ey = p.E[1];
+  const T *__restrict__ Ez = p.E[2];
+  T *__restrict__ Bx = p.B[0];
+  T *__restrict__ By = p.B[1];
+  T *__restrict__ Bz = p.B[2];
+  T ikx[V];
+#pragma unroll
+  for (int c = 0; c < V; ++c) ikx[c] = ld(p.ik[0] + i0 + c + 1);
+  const T iky = ld(p.ik[1] + j + 1);
+  const T iky_bz = ld(p.ik_bz_y + j + 1);
+  // y faces (slots 0, 1) hold whole rows: warp-uniform; x faces (slots 2, 3)
+  // per cell, bits 2c and 2c + 1
+  const unsigned ybits = face_column_mask(p.cpml, i0, j) & 3u;
+  unsigned xbits = 0;
+#pragma unroll
+  for (int c = 0; c < V; ++c) xbits |= ((face_column_mask(p.cpml, i0 + c, j) >> 2) & 3u) << (2 * c);
+  const int2 srck = source_plane_range(p);
+
+  RowV<T> ex = ldv(Ex + (long long)k0 * plane + col), ey = ldv(Ey + (long long)k0 * plane + col);
+  for (int k = k0; k <= k1; ++k) {
+    const long long base = (long long)k * plane;
+    int kp = k + 1;
+    if (p.zperiodic && kp == p.nz + 1) kp = 1;
+    const long long basep = (long long)kp * plane;
+    // ---- every load of this plane first
+    const RowV<T> ex_kp = ldv(Ex + basep + col), ey_kp = ldv(Ey + basep + col);
+    const RowV<T> ez = ldv(Ez + base + col);
+    const T ez_xl = ld(Ez + base + colxl), ey_xl = ld(Ey + base + colxl);
+    const RowV<T> ez_yp = ldv(Ez + base + colyp), ex_yp = ldv(Ex + base + colyp);
+    const RowV<T> bx = ldv_rw(Bx + base + col), by = ldv_rw(By + base + col), bz = ldv_rw(Bz + base + col);
+    const T ikz = ld(p.ik[2] + k);
+    // ---- H-side currents, in MPulse's order: faces by slot, then the injector
+    T m[V][3];
+#pragma unroll
+    for (int c = 0; c < V; ++c) m[c][0] = m[c][1] = m[c][2] = T(0);
+    if (ybits) {
+#pragma unroll
+      for (int c = 0; c < V; ++c) {
+        const T d0 = ex_yp.v[c] - ex.v[c], d1 = -(ez_yp.v[c] - ez.v[c]);
+        if (ybits & 1u) b_face<T, 0>(p, i0 + c, j, k, d0, d1, m[c]);
+        if (ybits & 2u) b_face<T, 1>(p, i0 + c, j, k, d0, d1, m[c]);
+      }
+    }
+    if (xbits) {
+#pragma unroll
+      for (int c = 0; c < V; ++c) {
+        const T ezx = c + 1 < V ? ez.v[c + 1 < V ? c + 1 : 0] : ez_xl;
+        const T eyx = c + 1 < V ? ey.v[c + 1 < V ? c + 1 : 0] : ey_xl;
+        const T d0 = ezx - ez.v[c], d1 = -(eyx - ey.v[c]);
+        if (xbits & (1u << (2 * c))) b_face<T, 2>(p, i0 + c, j, k, d0, d1, m[c]);
+        if (xbits & (2u << (2 * c))) b_face<T, 3>(p, i0 + c, j, k, d0, d1, m[c]);
+      }
+    }
+    if (z_face_plane(p.cpml, k)) {
+      const bool z4 = p.cpml[4].active && k >= p.cpml[4].lo && k <= p.cpml[4].hi;
+      const bool z5 = p.cpml[5].active && k >= p.cpml[5].lo && k <= p.cpml[5].hi;
+#pragma unroll
+      for (int c = 0; c < V; ++c) {
+        const T d0 = ey_kp.v[c] - ey.v[c], d1 = -(ex_kp.v[c] - ex.v[c]);
+        if (z4) b_face<T, 4>(p, i0 + c, j, k, d0, d1, m[c]);
+        if (z5) b_face<T, 5>(p, i0 + c, j, k, d0, d1, m[c]);
+      }
+    }
+    if (k >= srck.x && k <= srck.y) {
+      for (int s = 0; s < p.n_src; ++s) {
+        if (k != p.src[s].plane) continue;
+#pragma unroll
+        for (int c = 0; c < V; ++c) {
+          const T sa = ld(p.src[s].v0 + col + c), sb = ld(p.src[s].v1 + col + c);
+          for (int q = 0; q < p.src_mult; ++q) {
+            m[c][0] += sa;
+            m[c][1] += sb;
+          }
+        }
+      }
+    }
+    // ---- plrcStepB (fdtd_plrc.cpp:263-293)
+    const T dt = p.dt;
+    RowV<T> bxn, byn, bzn;
+#pragma unroll
+    for (int c = 0; c < V; ++c) {
+      const T ezx = c + 1 < V ? ez.v[c + 1 < V ? c + 1 : 0] : ez_xl;
+      const T eyx = c + 1 < V ? ey.v[c + 1 < V ? c + 1 : 0] : ey_xl;
+      bxn.v[c] = bx.v[c] + dt * ((ey_kp.v[c] - ey.v[c]) * ikz - (ez_yp.v[c] - ez.v[c]) * iky + m[c][0]);
+      byn.v[c] = by.v[c] + dt * ((ezx - ez.v[c]) * ikx[c] - (ex_kp.v[c] - ex.v[c]) * ikz + m[c][1]);
+      bzn.v[c] = bz.v[c] + dt * ((ex_yp.v[c] - ex.v[c]) * iky_bz - (eyx - ey.v[c]) * ikx[c] + m[c][2]);
+    }
+    stv(Bx + base + col, bxn);
+    stv(By + base + col, byn);
+    stv(Bz + base + col, bzn);
+    ex = ex_kp;
+    ey = ey_kp;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers (called from mp_api.cu)
 
@@ -248,6 +432,15 @@ cudaError_t launch_e_half(const EParams<T> &p, int mode, int np, cudaStream_t st
 template <typename T>
 cudaError_t launch_b_half(const BParams<T> &p, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
+#if MPB_B_VECTOR
+  constexpr int V = 16 / sizeof(T);
+  if (p.nx % V == 0) {
+    const int tx = p.nx / V;
+    const dim3 g((tx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk);
+    b_half_vec_kernel<T><<<g, dim3(32, MPB_B_BLOCK_Y, 1), 0, st>>>(p);
+    return cudaGetLastError();
+  }
+#endif
   const dim3 g((p.nx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk);
   b_half_kernel<T><<<g, dim3(32, MPB_B_BLOCK_Y, 1), 0, st>>>(p);
   return cudaGetLastError();

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
 }
 
 // The B half with 16-byte loads along x: each thread owns V = 16 / sizeof(T)
-// consecutive cells of a row (nx a multiple of V), so a plane's loads are 8
+// consecutive cells of a row (nx a multiple of 32 V), so a plane's loads are 8
 // vectors and two scalars (the x+1 neighbour of the last cell) per V cells,
 // and the z+1 plane of E is carried to the next plane.  Cells of warps or
 // planes with a CPML face or an injection plane go through b_cell one by one.
@@ -442,13 +442,16 @@ cudaError_t launch_b_half(const BParams<T> &p, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
 #if MPB_B_VECTOR
   constexpr int V = 16 / sizeof(T);
-  if (p.nx % V == 0) {
-    // V cells per thread: z-chunks sized for about MPB_BV_BLOCKS_PER_SM blocks per SM
+  // rows of whole warps only: on narrow grids (nx = 96: 24 threads a row)
+  // the scalar kernel keeps every lane busy
+  if (p.nx % (32 * V) == 0) {
+    // V cells per thread: z-chunks sized for about MPB_BV_BLOCKS_PER_SM blocks
+    // per SM, at least 8 planes each
     const int tx = p.nx / V;
-    const long long bxy = (long long)((tx + 31) / 32) * ((p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y);
+    const long long bxy = (long long)(tx / 32) * ((p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y);
     const long long chunks = std::max(1LL, (148LL * MPB_BV_BLOCKS_PER_SM + bxy - 1) / bxy);
     BParams<T> q = p;
-    q.kchunk = int(std::max(1LL, (nk + chunks - 1) / chunks));
+    q.kchunk = int(std::max(8LL, (nk + chunks - 1) / chunks));
     const dim3 g((tx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + q.kchunk - 1) / q.kchunk);
     b_half_vec_kernel<T><<<g, dim3(32, MPB_B_BLOCK_Y, 1), 0, st>>>(q);
     return cudaGetLastError();

@@ -44,21 +44,31 @@
 #ifndef MPB_B_MIN_THREADS
 #define MPB_B_MIN_THREADS 768
 #endif
-// B half: issue the next plane's loads before the current plane's arithmetic.
-// B half: 16-byte loads along x where nx allows, with its own occupancy and
-// z-chunks (four cells per thread: a quarter of the threads).  Measured on the
-// 256x256x512 workload: 640 resident threads and the scalar kernel's chunks
-// 0.419 ms, 768 threads (68 B spilled) and chunks for 8 / 16 / 24 blocks per
-// SM 0.387 / 0.358 / 0.354 ms, 896 threads 0.375 ms.
+// B half: two cells per thread with vector loads along x where nx allows,
+// with its own occupancy and z-chunks (half the threads), per precision.
+// Measured on the 256x256x512 workload (FP32, B half): scalar kernel 0.440
+// ms; four cells per thread (float4), 768 threads, chunks for 24 blocks per SM
+// 0.354 ms; two cells per thread (float2) with 768 / 1024 / 1280 / 1536
+// threads 0.335 / 0.293 / 0.304 / 0.302 ms, 1024 threads and 32 blocks per SM
+// 0.290 ms.  FP64 (double2), B half with 512 / 640 / 768 / 1024 threads:
+// 0.553 / 0.488 / 0.538 / 0.560 ms.
 #ifndef MPB_B_VECTOR
 #define MPB_B_VECTOR 1
 #endif
-#ifndef MPB_BV_MIN_THREADS
-#define MPB_BV_MIN_THREADS 768
+#ifndef MPB_BV_MIN_THREADS_F
+#define MPB_BV_MIN_THREADS_F 1024
 #endif
-#ifndef MPB_BV_BLOCKS_PER_SM
-#define MPB_BV_BLOCKS_PER_SM 24
+#ifndef MPB_BV_MIN_THREADS_D
+#define MPB_BV_MIN_THREADS_D 640
 #endif
+#ifndef MPB_BV_BLOCKS_PER_SM_F
+#define MPB_BV_BLOCKS_PER_SM_F 32
+#endif
+#ifndef MPB_BV_BLOCKS_PER_SM_D
+#define MPB_BV_BLOCKS_PER_SM_D 24
+#endif
+// B half, scalar kernel: issue the next plane's loads before the current
+// plane's arithmetic.
 #ifndef MPB_B_PREFETCH
 #define MPB_B_PREFETCH 1
 #endif
@@ -228,23 +238,25 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
   }
 }
 
-// The B half with 16-byte loads along x: each thread owns V = 16 / sizeof(T)
-// consecutive cells of a row (nx a multiple of 32 V), so a plane's loads are 8
-// vectors and two scalars (the x+1 neighbour of the last cell) per V cells,
-// and the z+1 plane of E is carried to the next plane.  Cells of warps or
-// planes with a CPML face or an injection plane go through b_cell one by one.
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { typedef float4 type; };
-template <> struct Vec16<double> { typedef double2 type; };
+// The B half with vector loads along x: each thread owns V = 2 consecutive
+// cells of a row (nx a multiple of 64), so a plane's loads are 8 float2 /
+// double2 vectors and two scalars (the x+1 neighbour of the second cell), and
+// the z+1 plane of E is carried to the next plane.  The CPML faces add their
+// currents cell by cell (y faces hold whole rows, x faces single cells, z
+// faces whole planes).
+template <typename T> struct VecB;
+template <> struct VecB<float> { typedef float2 type; };
+template <> struct VecB<double> { typedef double2 type; };
+constexpr int kBV = 2;  // cells per thread
 
 template <typename T>
 struct RowV {
-  T v[16 / sizeof(T)];
+  T v[kBV];
 };
 
 template <typename T>
 __device__ __forceinline__ RowV<T> ldv(const T *p) {
-  typedef typename Vec16<T>::type VT;
+  typedef typename VecB<T>::type VT;
   const VT x = __ldg(reinterpret_cast<const VT *>(p));
   RowV<T> r;
   memcpy(r.v, &x, sizeof(VT));
@@ -253,7 +265,7 @@ __device__ __forceinline__ RowV<T> ldv(const T *p) {
 
 template <typename T>
 __device__ __forceinline__ RowV<T> ldv_rw(const T *p) {
-  typedef typename Vec16<T>::type VT;
+  typedef typename VecB<T>::type VT;
   const VT x = *reinterpret_cast<const VT *>(p);
   RowV<T> r;
   memcpy(r.v, &x, sizeof(VT));
@@ -262,7 +274,7 @@ __device__ __forceinline__ RowV<T> ldv_rw(const T *p) {
 
 template <typename T>
 __device__ __forceinline__ void stv(T *p, const RowV<T> &r) {
-  typedef typename Vec16<T>::type VT;
+  typedef typename VecB<T>::type VT;
   VT x;
   memcpy(&x, r.v, sizeof(VT));
   *reinterpret_cast<VT *>(p) = x;
@@ -292,9 +304,10 @@ __device__ __forceinline__ void b_face(const BParams<T> &p, int i, int j, int k,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_BV_MIN_THREADS / (32 * MPB_B_BLOCK_Y))
+__global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
+                                  (sizeof(T) == 4 ? MPB_BV_MIN_THREADS_F : MPB_BV_MIN_THREADS_D) / (32 * MPB_B_BLOCK_Y))
     b_half_vec_kernel(const BParams<T> p) {
-  constexpr int V = 16 / sizeof(T);
+  constexpr int V = kBV;
   const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i0 >= p.nx || j >= p.ny) return;
@@ -441,15 +454,16 @@ template <typename T>
 cudaError_t launch_b_half(const BParams<T> &p, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
 #if MPB_B_VECTOR
-  constexpr int V = 16 / sizeof(T);
-  // rows of whole warps only: on narrow grids (nx = 96: 24 threads a row)
+  constexpr int V = kBV;
+  // rows of whole warps only: on narrow grids (nx = 96: 48 threads a row)
   // the scalar kernel keeps every lane busy
   if (p.nx % (32 * V) == 0) {
-    // V cells per thread: z-chunks sized for about MPB_BV_BLOCKS_PER_SM blocks
-    // per SM, at least 8 planes each
+    // V cells per thread: z-chunks sized for a number of blocks per SM, at
+    // least 8 planes each
     const int tx = p.nx / V;
+    const long long per_sm = sizeof(T) == 4 ? MPB_BV_BLOCKS_PER_SM_F : MPB_BV_BLOCKS_PER_SM_D;
     const long long bxy = (long long)(tx / 32) * ((p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y);
-    const long long chunks = std::max(1LL, (148LL * MPB_BV_BLOCKS_PER_SM + bxy - 1) / bxy);
+    const long long chunks = std::max(1LL, (148LL * per_sm + bxy - 1) / bxy);
     BParams<T> q = p;
     q.kchunk = int(std::max(8LL, (nk + chunks - 1) / chunks));
     const dim3 g((tx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + q.kchunk - 1) / q.kchunk);

@@ -103,6 +103,17 @@ struct mp_ctx {
   int src_plane[MP_MAX_SOURCES][2];
   void *src_buf = nullptr;   // injection planes of up to src_batch steps
   int src_batch = 1;
+  // Source batches computed ahead (every injector but gauss_inject): buffer b
+  // (src_buf, src_buf2) holds the planes of steps [pre_t0[b], pre_t0[b] +
+  // pre_k[b]); while one is stepped, the next batch is computed into the other
+  // on src_stream, so the FP64 source arithmetic overlaps the step kernels.
+  void *src_buf2 = nullptr;
+  cudaStream_t src_stream = nullptr;
+  cudaEvent_t src_done[2] = {nullptr, nullptr};  // the side stream's write of buffer b is done
+  cudaEvent_t src_free[2] = {nullptr, nullptr};  // the steps reading buffer b are done
+  long long pre_t0[2] = {0, 0};
+  int pre_k[2] = {0, 0};
+  bool pre_pending[2] = {false, false};  // a side-stream write of buffer b may be in flight
   GaussBeam *gauss = nullptr;  // gauss_inject state when the last injector is one
   double *d_wcoef = nullptr;
   int *d_status = nullptr;
@@ -662,6 +673,14 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
     const size_t per_step = 4 * size_t(c->plane) * c->esz;
     c->src_batch = int(std::max<size_t>(1, std::min<size_t>(64, (size_t(256) << 20) / per_step)));
     MPB_TRY(dalloc(c, &c->src_buf, size_t(c->src_batch) * per_step), "source allocation");
+    if (!c->gauss) {
+      MPB_TRY(dalloc(c, &c->src_buf2, size_t(c->src_batch) * per_step), "source allocation");
+      MPB_TRY(cudaStreamCreateWithFlags(&c->src_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      for (int b = 0; b < 2; ++b) {
+        MPB_TRY(cudaEventCreateWithFlags(&c->src_done[b], cudaEventDisableTiming), "cudaEventCreate");
+        MPB_TRY(cudaEventCreateWithFlags(&c->src_free[b], cudaEventDisableTiming), "cudaEventCreate");
+      }
+    }
   }
 
   // upload the lines
@@ -807,18 +826,80 @@ struct StepHooks {
   std::function<int(long long)> before, after;
 };
 
+// The injection planes of the steps from c->time on, from the buffers that
+// src_stream fills ahead; launches the next batch into the other buffer.
+// Returns the planes of step c->time in *planes and the steps they cover.
+template <typename T>
+int sources_ahead(mp_ctx *c, int want, const T **planes, int *steps) {
+  T *bufs[2] = {static_cast<T *>(c->src_buf), static_cast<T *>(c->src_buf2)};
+  const size_t per_step = 4 * size_t(c->plane);
+  cudaError_t e;
+  int u = -1;
+  for (int b = 0; b < 2; ++b)
+    if (c->pre_k[b] > 0 && c->time >= c->pre_t0[b] && c->time < c->pre_t0[b] + c->pre_k[b]) u = b;
+  if (u < 0) {
+    // nothing ahead covers this step: compute a batch here, into buffer 0
+    u = 0;
+    if (c->pre_pending[0] && (e = cudaStreamWaitEvent(c->stream, c->src_done[0], 0)) != cudaSuccess)
+      return cuda_err(c, e, "cudaStreamWaitEvent");
+    e = launch_source_batch<T>(c->sq[0][0], c->sq[0][1], c->time, c->src_batch, bufs[0], c->stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
+    c->launches++;
+    c->pre_t0[0] = c->time;
+    c->pre_k[0] = c->src_batch;
+    c->pre_pending[0] = false;
+  } else if (c->pre_pending[u]) {
+    if ((e = cudaStreamWaitEvent(c->stream, c->src_done[u], 0)) != cudaSuccess)
+      return cuda_err(c, e, "cudaStreamWaitEvent");
+    c->pre_pending[u] = false;
+  }
+  const int off = int(c->time - c->pre_t0[u]);
+  *planes = bufs[u] + size_t(off) * per_step;
+  *steps = std::min(want, c->pre_k[u] - off);
+  // the batch after this buffer's, into the other one once the steps that
+  // read it (all launched before now) are done
+  const int w = 1 - u;
+  const long long nt0 = c->pre_t0[u] + c->pre_k[u];
+  if (!(c->pre_k[w] > 0 && c->pre_t0[w] == nt0)) {
+    if ((e = cudaEventRecord(c->src_free[w], c->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(c->src_stream, c->src_free[w], 0)) != cudaSuccess)
+      return cuda_err(c, e, "event");
+    e = launch_source_batch<T>(c->sq[0][0], c->sq[0][1], nt0, c->src_batch, bufs[w], c->src_stream);
+    if (e != cudaSuccess) return cuda_err(c, e, "source kernel");
+    if ((e = cudaEventRecord(c->src_done[w], c->src_stream)) != cudaSuccess) return cuda_err(c, e, "event");
+    c->launches++;
+    c->pre_t0[w] = nt0;
+    c->pre_k[w] = c->src_batch;
+    c->pre_pending[w] = true;
+  }
+  return MP_OK;
+}
+
 // Per step: E half, B half.  The injection planes of a block of up to
 // src_batch steps are computed ahead in one launch (they depend on
 // Process::time only), and each half step reads its step's plane pair.
+// Without gauss_inject and the per-kernel timer the next block is computed on
+// a second stream while the current one is stepped (sources_ahead).
 template <typename T>
 int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer *tm = nullptr,
               double *acc = nullptr, const StepHooks *hooks = nullptr) {
   const size_t pl = size_t(c->plane);
+  const bool ahead = c->src_stream && !tm;
   int t = 0;
   while (t < n_steps) {
     int K = c->nsrc ? std::min(c->src_batch, n_steps - t) : n_steps - t;
     cudaError_t e;
-    if (c->nsrc) {
+    const T *planes = static_cast<const T *>(c->src_buf);
+    if (c->nsrc && ahead) {
+      NvtxRange nv("mp sources");
+      const int rc = sources_ahead<T>(c, K, &planes, &K);
+      if (rc != MP_OK) return rc;
+    } else if (c->nsrc) {
+      // computed here into buffer 0: what the buffers held ahead is void
+      if (c->pre_pending[0] && (e = cudaStreamWaitEvent(c->stream, c->src_done[0], 0)) != cudaSuccess)
+        return cuda_err(c, e, "cudaStreamWaitEvent");
+      c->pre_k[0] = c->pre_k[1] = 0;
+      c->pre_pending[0] = false;
       NvtxRange nv("mp sources");
       if (tm) cudaEventRecord(tm->ev[4], c->stream);
       if (c->gauss) {
@@ -848,7 +929,7 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
     }
     for (int q = 0; q < K; ++q) {
       if (c->nsrc) {
-        const T *base = static_cast<const T *>(c->src_buf) + size_t(q) * 4 * pl;
+        const T *base = planes + size_t(q) * 4 * pl;
         ep.src[0].v0 = base;
         ep.src[0].v1 = base + pl;
         bp.src[0].v0 = base + 2 * pl;
@@ -964,6 +1045,14 @@ void mp_destroy(mp_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->src_stream) {
+    cudaStreamSynchronize(c->src_stream);
+    cudaStreamDestroy(c->src_stream);
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (c->src_done[b]) cudaEventDestroy(c->src_done[b]);
+    if (c->src_free[b]) cudaEventDestroy(c->src_free[b]);
+  }
   for (void *p : c->allocs) cudaFree(p);
   if (c->gauss) {
     gauss_destroy(*c->gauss);

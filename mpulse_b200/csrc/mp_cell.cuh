@@ -25,7 +25,10 @@ template <> struct Vec2<double> { typedef double2 type; };
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 
-__device__ __forceinline__ bool finite3(double a, double b, double c) {
+// A value is finite in T exactly when it is finite after widening: test it
+// in T (no conversions in the FP32 form).
+template <typename T>
+__device__ __forceinline__ bool finite3(T a, T b, T c) {
   return isfinite(a) && isfinite(b) && isfinite(c);
 }
 
@@ -249,9 +252,10 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     const double D = sqrt((double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz);
     if (D > 0) {
       const double E = nl_newton(sqrt(E2), p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status);
-      exn = T(E * Dx / D);
-      eyn = T(E * Dy / D);
-      ezn = T(E * Dz / D);
+      const double sc = E / D;  // one division: E * D_c / D up to rounding
+      exn = T(sc * Dx);
+      eyn = T(sc * Dy);
+      ezn = T(sc * Dz);
     } else {
       exn = eyn = ezn = T(0);
     }
@@ -295,15 +299,16 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       const double C = sqrt((double)cx * cx + (double)cy * cy + (double)cz * cz);
       if (C > 0) {
         const double E = kerr_newton(sqrt(E2), lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
-        exn = T(E * cx / C);
-        eyn = T(E * cy / C);
-        ezn = T(E * cz / C);
+        const double sc = E / C;  // one division: E * c_c / |c| up to rounding
+        exn = T(sc * cx);
+        eyn = T(sc * cy);
+        ezn = T(sc * cz);
       } else {
         exn = eyn = ezn = T(0);
       }
     }
   }
-  if (!finite3((double)exn, (double)eyn, (double)ezn)) atomicAdd(p.status + ST_NONFINITE, 1);
+  if (!finite3(exn, eyn, ezn)) atomicAdd(p.status + ST_NONFINITE, 1);
   // ---- CPML stores
 #pragma unroll
   for (int f = 0; f < 6; ++f) {

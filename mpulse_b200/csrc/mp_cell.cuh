@@ -249,10 +249,13 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
     const T f = T(p.eps_d + p.chi_d * E2);
     const T Dx = f * ex + dt * cbx, Dy = f * ey + dt * cby, Dz = f * ez + dt * cbz;
-    const double D = sqrt((double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz);
-    if (D > 0) {
-      const double E = nl_newton(sqrt(E2), p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status);
-      const double sc = E / D;  // one division: E * D_c / D up to rounding
+    const double D2 = (double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz;
+    if (D2 > 0) {
+      const double rD = rsqrt(D2);  // as in the PLRC Kerr update below
+      const double D = D2 * rD;
+      const double E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
+      const double E = nl_newton(E0, p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status);
+      const double sc = E * rD;
       exn = T(sc * Dx);
       eyn = T(sc * Dy);
       ezn = T(sc * Dz);
@@ -296,10 +299,15 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       const T cx = (f * ex + dt * (cbx + jx) + Px) * lc.inv_denom;
       const T cy = (f * ey + dt * (cby + jy) + Py) * lc.inv_denom;
       const T cz = (f * ez + dt * (cbz + jz) + Pz) * lc.inv_denom;
-      const double C = sqrt((double)cx * cx + (double)cy * cy + (double)cz * cz);
-      if (C > 0) {
-        const double E = kerr_newton(sqrt(E2), lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
-        const double sc = E / C;  // one division: E * c_c / |c| up to rounding
+      // |c|, 1/|c| and the start |E^n| from reciprocal square roots: no FP64
+      // square root or division here (equal to sqrt and / up to rounding)
+      const double C2 = (double)cx * cx + (double)cy * cy + (double)cz * cz;
+      if (C2 > 0) {
+        const double rC = rsqrt(C2);
+        const double C = C2 * rC;
+        const double E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
+        const double E = kerr_newton(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
+        const double sc = E * rC;
         exn = T(sc * cx);
         eyn = T(sc * cy);
         ezn = T(sc * cz);

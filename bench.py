@@ -289,7 +289,7 @@ def run_adjoint(local_rank: int) -> dict:
     """The adjoint workload (96^3, single-pole medium, 32^3 design region,
     1500 steps, |E|^2 monitor objective): wall time of the forward run that
     computes J (mp_objective) and of mp_adjoint (forward with checkpoints +
-    reverse pass), best of two; FP32 with a checkpoint every 50 steps (the
+    reverse pass), best of three; FP32 with a checkpoint every 50 steps (the
     workload's schedule) and with the whole E history kept, and the FP32
     gradient against the FP64 one."""
     from mpulse_b200 import runtime
@@ -310,7 +310,7 @@ def run_adjoint(local_rank: int) -> dict:
 
         def timed(fn):
             best, res = None, None
-            for _ in range(2):
+            for _ in range(3):
                 with fresh() as g:
                     t0 = time.perf_counter()
                     res = fn(g)

@@ -113,6 +113,40 @@ def test_time_counter_and_sources_follow_process_time():
             assert rel_l2(g.download(n), o.download(n)) <= TOL_FP64
 
 
+@pytest.mark.parametrize("precision,tol", [(abi.MP_FP64, TOL_FP64), (abi.MP_FP32, TOL_FP32)])
+def test_sources_computed_ahead_follow_single_steps_and_time_jumps(precision, tol):
+    """The injection planes are computed a batch ahead on a second stream, in
+    buffers keyed by the steps they hold.  Single steps across a batch
+    boundary (the batch is 64 steps here), a jump back in time and a jump
+    forward past both buffers give the oracle's fields."""
+    cfg = make_case("lin_split_cpmlz_gauss", precision)
+    cfg64 = make_case("lin_split_cpmlz_gauss", abi.MP_FP64)
+    init = random_fields(cfg64, seed=17, smooth=True, scale=0.05)
+    o = pyoracle.OracleSim(cfg64)
+    for n, v in init.items():
+        o.upload(n, v)
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        for _ in range(70):  # one step per call, across the first batch boundary
+            g.step(1)
+        assert o.step(70) == abi.MP_OK
+        for n in abi.FIELD_NAMES:
+            assert rel_l2(g.download(n), o.download(n)) <= tol, n
+        g.time = 30  # back into the first batch
+        o.time = 30
+        g.step(50)
+        assert o.step(50) == abi.MP_OK
+        for n in abi.FIELD_NAMES:
+            assert rel_l2(g.download(n), o.download(n)) <= tol, n
+        g.time = 400  # beyond both buffers
+        o.time = 400
+        g.step(5)
+        assert o.step(5) == abi.MP_OK
+        for n in abi.FIELD_NAMES:
+            assert rel_l2(g.download(n), o.download(n)) <= tol, n
+
+
 @pytest.mark.parametrize("start,steps", [(21, 30), (0, 60), (45, 8)])
 def test_gauss_beam_blocks_follow_process_time(start, steps):
     """gauss_inject with Nt = 16 and t_size = 40: blocks start at 0, 16, 32 and

@@ -71,6 +71,20 @@ __device__ __forceinline__ int2 source_plane_range(const P &p) {
   return r;
 }
 
+// 1/d for 1e-30 < d < 1e30: a single-precision estimate refined by two
+// Newton-Raphson steps r <- r + r (1 - d r) in FP64, each squaring the relative
+// error (the Newton-Raphson iteration for the reciprocal, e.g. Muller et al.,
+// Handbook of Floating-Point Arithmetic): about 1e-7, then 1e-14, then below
+// FP64 rounding.  Other d (a diverging field) fall back to the division.  The
+// Newton denominators below are at least 1 (Kerr) or eps (FDTD_Nonlinear).
+__device__ __forceinline__ double rcp_pos(double d) {
+  if (!(d > 1e-30 && d < 1e30)) return 1.0 / d;
+  double r = (double)__fdividef(1.0f, (float)d);
+  r = fma(r, fma(-d, r, 1.0), r);
+  r = fma(r, fma(-d, r, 1.0), r);
+  return r;
+}
+
 // Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
 // (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped.
 __device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
@@ -80,7 +94,7 @@ __device__ __forceinline__ double kerr_newton(double E, double A, double C, doub
   do {
     Eold = E;
     const double E2 = E * E;
-    E = (2.0 * A * E2 * E + C) / (3.0 * A * E2 + 1.0);
+    E = (2.0 * A * E2 * E + C) * rcp_pos(3.0 * A * E2 + 1.0);
   } while (fabs(E - Eold) > tol && ++it < maxit);
   if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
   return E;
@@ -94,7 +108,7 @@ __device__ __forceinline__ double nl_newton(double E, double eps, double chi, do
   do {
     Eold = E;
     const double E2 = E * E;
-    E = (2.0 * chi * E2 * E + D) / (3.0 * chi * E2 + eps);
+    E = (2.0 * chi * E2 * E + D) * rcp_pos(3.0 * chi * E2 + eps);
   } while (fabs(E - Eold) > tol && ++it < maxit);
   if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
   return E;

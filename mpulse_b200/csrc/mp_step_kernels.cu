@@ -49,8 +49,8 @@
 // Measured on the 256x256x512 workload (FP32, B half): scalar kernel 0.440
 // ms; four cells per thread (float4), 768 threads, chunks for 24 blocks per SM
 // 0.354 ms; two cells per thread (float2) with 768 / 1024 / 1280 / 1536
-// threads 0.335 / 0.293 / 0.304 / 0.302 ms, 1024 threads and 32 blocks per SM
-// 0.290 ms.  FP64 (double2), B half with 512 / 640 / 768 / 1024 threads:
+// threads 0.335 / 0.293 / 0.304 / 0.302 ms, 1024 threads and 32 / 48 blocks
+// per SM 0.290 / 0.285 ms (32 x 2 blocks: 0.284 ms, 32 x 8: 0.307 ms).  FP64 (double2), B half with 512 / 640 / 768 / 1024 threads:
 // 0.553 / 0.488 / 0.538 / 0.560 ms.
 #ifndef MPB_B_VECTOR
 #define MPB_B_VECTOR 1
@@ -62,7 +62,7 @@
 #define MPB_BV_MIN_THREADS_D 640
 #endif
 #ifndef MPB_BV_BLOCKS_PER_SM_F
-#define MPB_BV_BLOCKS_PER_SM_F 32
+#define MPB_BV_BLOCKS_PER_SM_F 48
 #endif
 #ifndef MPB_BV_BLOCKS_PER_SM_D
 #define MPB_BV_BLOCKS_PER_SM_D 24

@@ -243,13 +243,13 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       // background: E' = (eps_bg E + dt (curl + J)) / eps_bg
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        g[c] = a[c] * R(p.inv_eps_bg);
-        ne[c] = R(p.eps_bg) * g[c];
+        g[c] = a[c] * p.inv_eps_bg_t;
+        ne[c] = p.eps_bg_t * g[c];
       }
     } else {
       const double dD = p.sumChi0 - p.sumXi0;
       double denom = 0.0, A = p.A0;
-      R idn = R(p.inv_denom0), numer = R(p.numer0), Rchi = R(p.nonlin ? p.chi : 0.0);
+      R idn = p.inv_denom0_t, numer = p.numer0_t, Rchi = p.chi_nl_t;
       if (dcell) {
         denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
         A = p.nonlin ? u * p.chi / denom : 0.0;
@@ -285,12 +285,12 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       for (int c = 0; c < 3; ++c) ne[c] = f * g[c] + R(2) * Rchi * En[c] * Eg;
       // reverse PLRC recursion: psi~bar = conj(Crec) psibar + g
       double gs = 0.0;
-      const R Rs = R(s);
+      const R Rs = dcell ? R(s) : R(1);
 #pragma unroll
       for (int n = 0; n < NP; ++n) {
-        const R Dr = R(p.pD[n][0]), Di = R(p.pD[n][1]);
-        const R Xr = R(p.pxi[n][0]), Xi = R(p.pxi[n][1]);
-        const R Cr = R(p.pC[n][0]), Ci = R(p.pC[n][1]);
+        const R Dr = p.pDt[n][0], Di = p.pDt[n][1];
+        const R Xr = p.pxit[n][0], Xi = p.pxit[n][1];
+        const R Cr = p.pCt[n][0], Ci = p.pCt[n][1];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const R pr = pq[n][c][0], pim = pq[n][c][1];
@@ -335,11 +335,11 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       if (p.obj_kind == 1) {
         if (k >= p.oz0 && k <= p.oz1) {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) ne[c] += R(p.obj_f) * En[c];
+          for (int c = 0; c < 3; ++c) ne[c] += p.obj_f_t * En[c];
         }
       } else if (k == p.oz0) {
-        ne[0] += R(p.obj_f) * oby;
-        ne[1] -= R(p.obj_f) * obx;
+        ne[0] += p.obj_f_t * oby;
+        ne[1] -= p.obj_f_t * obx;
       }
     }
 
@@ -491,8 +491,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     zw_on = ezq >= 0;
     // the objective's B term of the state before the step (Sz plane)
     if (obj) {
-      b[0] -= R(p.obj_f) * oey;
-      b[1] += R(p.obj_f) * oex;
+      b[0] -= p.obj_f_t * oey;
+      b[1] += p.obj_f_t * oex;
     }
 
     // ---- stores: B adjoint, H-face totals for the step before (b * total + dt * B adjoint)

@@ -1701,6 +1701,18 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   objective_box(a, b0);
   p.ox0 = b0[0]; p.ox1 = b0[1]; p.oy0 = b0[2]; p.oy1 = b0[3]; p.oz0 = b0[4]; p.oz1 = b0[5];
   p.obj_f = a->kind == MP_OBJ_E2_BOX ? 2.0 * g.dt : g.dt * g.dx * g.dy;
+  for (int s = 0; s < 3; ++s)
+    for (int r = 0; r < 2; ++r) {
+      p.pDt[s][r] = T(p.pD[s][r]);
+      p.pxit[s][r] = T(p.pxi[s][r]);
+      p.pCt[s][r] = T(p.pC[s][r]);
+    }
+  p.inv_eps_bg_t = T(p.inv_eps_bg);
+  p.eps_bg_t = T(p.eps_bg);
+  p.numer0_t = T(p.numer0);
+  p.inv_denom0_t = T(p.inv_denom0);
+  p.chi_nl_t = T(p.nonlin ? p.chi : 0.0);
+  p.obj_f_t = T(p.obj_f);
 
   auto copy_state = [&](long long slot, bool save) -> cudaError_t {
     size_t off = 0;

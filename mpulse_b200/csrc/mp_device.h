@@ -163,6 +163,10 @@ struct AdjParams {
   double pD[3][2], pxi[3][2], pC[3][2];  // active poles, FP64
   double sumChi0, sumXi0, chi, eps, eps_bg;
   double inv_eps_bg, numer0, inv_denom0, A0;  // background and uniform-medium constants
+  // the same constants rounded to the state precision once (cells outside the
+  // design region use these; no per-cell conversions)
+  T pDt[3][2], pxit[3][2], pCt[3][2];
+  T inv_eps_bg_t, eps_bg_t, numer0_t, inv_denom0_t, chi_nl_t, obj_f_t;
   int np, mz0, mz1, nonlin;
   int kchunk_e, kchunk_b;  // planes per block of adj_e (1..nz) / adj_b (0..nz)
   AdjFace<T> fe[3], fh[3];  // per axis x, y, z

@@ -33,7 +33,7 @@
 #define MPB_ADJ_BLOCK_Y 4
 #endif
 #ifndef MPB_ADJ_E_MIN_F
-#define MPB_ADJ_E_MIN_F 512
+#define MPB_ADJ_E_MIN_F 640
 #endif
 #ifndef MPB_ADJ_E_MIN_D
 #define MPB_ADJ_E_MIN_D 512
@@ -120,21 +120,12 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   const T *Bx = p.Bb[0], *By = p.Bb[1], *Bz = p.Bb[2];
   const AdjFace<T> &HX = p.fh[0], &HY = p.fh[1], &HZ = p.fh[2];
   const AdjFace<T> &EX = p.fe[0], &EY = p.fe[1], &EZ = p.fe[2];
-  // H faces at this column and at x-1 / y-1; E faces at this column
-  const int hxo = face_pos(HX, i + 1), hxm = face_pos(HX, im + 1);
-  const int hyo = face_pos(HY, j + 1), hym = face_pos(HY, jm + 1);
-  const R hxco = hxo >= 0 ? R(HX.c[i + 1]) : R(0), hxcm = hxm >= 0 ? R(HX.c[im + 1]) : R(0);
-  const R hyco = hyo >= 0 ? R(HY.c[j + 1]) : R(0), hycm = hym >= 0 ? R(HY.c[jm + 1]) : R(0);
-  const int exo = face_pos(EX, i + 1), eyo = face_pos(EY, j + 1);
-  const R exb = exo >= 0 ? R(EX.b[i + 1]) : R(0), eyb = eyo >= 0 ? R(EY.b[j + 1]) : R(0);
   const int plane = int(pl);
-  const int chxo = face_col<0>(HX, hxo, i, j, nx), chxm = face_col<0>(HX, hxm, im, j, nx);
-  const int chyo = face_col<1>(HY, hyo, i, j, nx), chym = face_col<1>(HY, hym, i, jm, nx);
-  const int cexo = face_col<0>(EX, exo, i, j, nx), ceyo = face_col<1>(EY, eyo, i, j, nx);
   // warps whose columns lie in no x / y face skip the face code on planes
-  // outside the z faces
-  const bool warp_xy =
-      __any_sync(__activemask(), (hxo >= 0) || (hxm >= 0) || (hyo >= 0) || (hym >= 0) || (exo >= 0) || (eyo >= 0));
+  // outside the z faces; the face positions are recomputed where used
+  const bool warp_xy = __any_sync(__activemask(), (face_pos(HX, i + 1) >= 0) || (face_pos(HX, im + 1) >= 0) ||
+                                                      (face_pos(HY, j + 1) >= 0) || (face_pos(HY, jm + 1) >= 0) ||
+                                                      (face_pos(EX, i + 1) >= 0) || (face_pos(EY, j + 1) >= 0));
   // the z H face's c * total at plane k - 1, carried
   R cw0, cw1;
   bool cw_on;
@@ -194,17 +185,25 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     R ex0 = R(0), ex1 = R(0), ey0 = R(0), ey1 = R(0), ez0 = R(0), ez1 = R(0), ezb = R(0);
     int lexo = 0, leyo = 0, lezo = 0;
     if (fpl) {
+      const int hxo = face_pos(HX, i + 1), hxm = face_pos(HX, im + 1);
+      const int hyo = face_pos(HY, j + 1), hym = face_pos(HY, jm + 1);
+      const R hxco = hxo >= 0 ? R(HX.c[i + 1]) : R(0), hxcm = hxm >= 0 ? R(HX.c[im + 1]) : R(0);
+      const R hyco = hyo >= 0 ? R(HY.c[j + 1]) : R(0), hycm = hym >= 0 ? R(HY.c[jm + 1]) : R(0);
+      const int exo = face_pos(EX, i + 1), eyo = face_pos(EY, j + 1);
+      const int chxo = face_col<0>(HX, hxo, i, j, nx), chxm = face_col<0>(HX, hxm, im, j, nx);
+      const int chyo = face_col<1>(HY, hyo, i, j, nx), chym = face_col<1>(HY, hym, i, jm, nx);
+      const int cexo = face_col<0>(EX, exo, i, j, nx), ceyo = face_col<1>(EY, eyo, i, j, nx);
       const int shx = face_plane<0>(HX, k, nx, ny), shy = face_plane<1>(HY, k, nx, ny);
       face_w(HX, hxo, chxo + shx, hxco, hx0o, hx1o);
       face_w(HX, hxm, chxm + shx, hxcm, hx0m, hx1m);
       face_w(HY, hyo, chyo + shy, hyco, hy0o, hy1o);
       face_w(HY, hym, chym + shy, hycm, hy0m, hy1m);
       face_w(HZ, hzp, hzp * plane + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1);
-      lexo = cexo + face_plane<0>(EX, k, nx, ny);
-      leyo = ceyo + face_plane<1>(EY, k, nx, ny);
+      lexo = exo >= 0 ? cexo + face_plane<0>(EX, k, nx, ny) : -1;
+      leyo = eyo >= 0 ? ceyo + face_plane<1>(EY, k, nx, ny) : -1;
       lezo = ezp * plane + col;
-      if (exo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
-      if (eyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
+      if (lexo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
+      if (leyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
       if (ezp >= 0) { ez0 = EZ.a0[lezo]; ez1 = EZ.a1[lezo]; ezb = EZ.b[k]; }
     }
     R obx = R(0), oby = R(0);
@@ -360,11 +359,13 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     }
     // E-face totals of this cell: b * total + dt * G
     if (fpl) {
-      if (exo >= 0) {
+      if (lexo >= 0) {
+        const R exb = R(EX.b[i + 1]);
         EX.a0[lexo] = T(exb * ex0 + dt * comp0<0>(g));
         EX.a1[lexo] = T(exb * ex1 + dt * comp1<0>(g));
       }
-      if (eyo >= 0) {
+      if (leyo >= 0) {
+        const R eyb = R(EY.b[j + 1]);
         EY.a0[leyo] = T(eyb * ey0 + dt * comp0<1>(g));
         EY.a1[leyo] = T(eyb * ey1 + dt * comp1<1>(g));
       }

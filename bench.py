@@ -477,7 +477,7 @@ def reference_slabs(steps: int, warmup: int, procs: int) -> dict:
         env = dict(os.environ, MPULSE_REF_WARMUP=str(warmup))
         runs.append((subprocess.Popen([binary, os.path.join(d, "setup.dat"), d], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, env=env, text=True), c))
-    secs, cells = [], 0
+    secs, cells, rates = [], 0, []
     for pr, c in runs:
         outp, _ = pr.communicate()
         if pr.returncode != 0:
@@ -485,8 +485,10 @@ def reference_slabs(steps: int, warmup: int, procs: int) -> dict:
         r = json.loads(outp.strip().splitlines()[-1])
         secs.append(r["seconds"])
         cells += r["cells"]
+        rates.append(r["cells"] * steps / r["seconds"] / 1e9)
     t = max(secs)
-    return {"value": cells * steps / t / 1e9, "procs": procs, "cells": cells, "seconds": t, "nz_slab": nz_slab}
+    return {"value": cells * steps / t / 1e9, "procs": procs, "cells": cells, "seconds": t, "nz_slab": nz_slab,
+            "per_core": float(np.median(rates))}
 
 
 def cpu_baseline_sample(args) -> dict:
@@ -498,7 +500,9 @@ def cpu_baseline_sample(args) -> dict:
     r = reference_slabs(steps=2, warmup=1, procs=procs)
     return {"value": round(r["value"], 6), "unit": UNIT, "cores": r["procs"], "kind": "reference",
             "sample": f"MPulse reference build (-O3), full 256x256x512 workload as {r['procs']} independent "
-                      f"z-slabs of {r['nz_slab']} planes, 1 warm-up + 2 timed steps"}
+                      f"z-slabs of {r['nz_slab']} planes, 1 warm-up + 2 timed steps",
+            "per_core_value": round(r["per_core"], 6),
+            "per_core": "median rate of one slab process (the reference is single-threaded), measured while all ran"}
 
 
 def cpu_baseline_port() -> dict:

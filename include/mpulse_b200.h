@@ -69,7 +69,8 @@ typedef enum mp_status {
   MP_ERR_NEWTON = -4,       /* Kerr Newton solve did not converge in a cell */
   MP_ERR_NONFINITE = -5,    /* a field value became NaN or Inf */
   MP_ERR_UNSUPPORTED = -6,  /* the configuration names a part that is not built */
-  MP_ERR_NAME = -7          /* unknown field name */
+  MP_ERR_NAME = -7,         /* unknown field name */
+  MP_ERR_BOUNDS = -8        /* checked build only: a kernel index fell outside its array (access skipped) */
 } mp_status;
 
 typedef enum mp_precision { MP_FP64 = 0, MP_FP32 = 1 } mp_precision;

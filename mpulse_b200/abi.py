@@ -21,6 +21,7 @@ MP_ERR_NEWTON = -4
 MP_ERR_NONFINITE = -5
 MP_ERR_UNSUPPORTED = -6
 MP_ERR_NAME = -7
+MP_ERR_BOUNDS = -8
 
 STATUS_NAMES = {
     MP_OK: "MP_OK",
@@ -31,6 +32,7 @@ STATUS_NAMES = {
     MP_ERR_NONFINITE: "MP_ERR_NONFINITE",
     MP_ERR_UNSUPPORTED: "MP_ERR_UNSUPPORTED",
     MP_ERR_NAME: "MP_ERR_NAME",
+    MP_ERR_BOUNDS: "MP_ERR_BOUNDS",
 }
 
 MP_FP64, MP_FP32 = 0, 1

@@ -6,6 +6,12 @@ Every .cu file under csrc/ is compiled with nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` and linked into one shared
 library next to this file.  Objects go to csrc/_build/ and are rebuilt only
 when a source or header is newer.
+
+``build(checked=True)`` makes libmpulse_b200_checked.so from the same sources
+with -DMPB_CHECKED=1 (objects in csrc/_build_checked/): the step kernels test
+every state index against its array's size and report skipped accesses
+(MP_ERR_BOUNDS) instead of touching memory outside an array.  Select it with
+MPULSE_B200_LIB.
 """
 from __future__ import annotations
 
@@ -20,6 +26,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(CSRC, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libmpulse_b200.so")
+LIB_CHECKED = os.path.join(HERE, "libmpulse_b200_checked.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # cuFFT: the once-per-block spectral precompute of gauss_inject
@@ -43,25 +50,27 @@ def _newer(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, checked: bool = False) -> str:
+    bdir, lib = (BUILD + "_checked", LIB_CHECKED) if checked else (BUILD, LIB)
+    flags = NVCC_FLAGS + (["-DMPB_CHECKED=1"] if checked else [])
+    os.makedirs(bdir, exist_ok=True)
     headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
                glob.glob(os.path.join(INCLUDE, "*.h")))
     objs = []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if _newer(obj, [src, *headers, __file__]):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
+            cmd = [nvcc(), *ARCH, *flags, "-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    if _newer(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", *LINK_LIBS]
+    if _newer(lib, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-lcudart", *LINK_LIBS]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 def ptxas_report() -> str:
@@ -78,4 +87,4 @@ if __name__ == "__main__":
     if "--ptxas" in sys.argv:
         print(ptxas_report())
     else:
-        print(build(verbose=True))
+        print(build(verbose=True, checked="--checked" in sys.argv))

@@ -280,6 +280,7 @@ void fill_face(CpmlFace<T> &F, const LayerHost &L, const T *lines) {
   F.ey = L.ey;
   F.psi0 = static_cast<T *>(L.psi0);
   F.psi1 = static_cast<T *>(L.psi1);
+  F.n = int(L.n);
   F.b = lines + L.b_off;
   F.c = lines + L.c_off;
 }
@@ -352,6 +353,8 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
   }
   ep.status = c->d_status;
   bp.status = c->d_status;
+  ep.n_field = bp.n_field = (long long)c->fcount;
+  ep.n_psi = (long long)c->psi_cells;
   // planes per block: enough blocks to fill 148 SMs several times over
   const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
   const long long target = 148LL * 8;
@@ -1180,9 +1183,12 @@ int mp_check_status(mp_ctx *c) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_err(c, e, "status read");
   const int newton = c->h_status[ST_NEWTON], nonfin = c->h_status[ST_NONFINITE];
-  const int timeout = c->h_status[ST_TIMEOUT];
-  if (newton || nonfin || timeout) {
+  const int timeout = c->h_status[ST_TIMEOUT], bounds = c->h_status[ST_BOUNDS];
+  if (newton || nonfin || timeout || bounds) {
     cudaMemsetAsync(c->d_status, 0, ST_COUNT * sizeof(int), c->stream);
+    if (bounds)
+      return set_err(c, MP_ERR_BOUNDS, "%d state accesses fell outside their arrays and were skipped (checked build)",
+                     bounds);
     if (timeout)
       return set_err(c, MP_ERR_CUDA, "%d blocks gave up waiting for their TMA plane loads; the step is incomplete",
                      timeout);

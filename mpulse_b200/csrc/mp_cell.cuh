@@ -25,6 +25,40 @@ template <> struct Vec2<double> { typedef double2 type; };
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 
+// State accesses of the step kernels.  A checked build (MPB_CHECKED=1, the
+// library libmpulse_b200_checked.so) tests every element index against the
+// size of its array; an index outside is counted in the status word
+// (ST_BOUNDS, reported by mp_step as MP_ERR_BOUNDS) and the access is skipped,
+// a load reading 0, so nothing faults.  The default build compiles these to
+// plain accesses.
+#ifndef MPB_CHECKED
+#define MPB_CHECKED 0
+#endif
+__device__ __forceinline__ bool in_bounds(long long i, long long n, int *status) {
+#if MPB_CHECKED
+  if ((unsigned long long)i < (unsigned long long)n) return true;
+  atomicAdd(status + ST_BOUNDS, 1);
+  return false;
+#else
+  (void)i;
+  (void)n;
+  (void)status;
+  return true;
+#endif
+}
+template <typename T>
+__device__ __forceinline__ T ldg_c(const T *a, long long i, long long n, int *status) {
+  return in_bounds(i, n, status) ? __ldg(a + i) : T{};
+}
+template <typename T>
+__device__ __forceinline__ T ld_c(const T *a, long long i, long long n, int *status) {
+  return in_bounds(i, n, status) ? a[i] : T{};
+}
+template <typename T>
+__device__ __forceinline__ void st_c(T *a, long long i, long long n, int *status, T v) {
+  if (in_bounds(i, n, status)) a[i] = v;
+}
+
 // A value is finite in T exactly when it is finite after widening: test it
 // in T (no conversions in the FP32 form).
 template <typename T>
@@ -208,8 +242,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
       else if (face_axis(f) == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
       else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
-      cp0[f] = F.psi0[cli[f]];
-      cp1[f] = F.psi1[cli[f]];
+      cp0[f] = ld_c(F.psi0, cli[f], F.n, p.status);
+      cp1[f] = ld_c(F.psi1, cli[f], F.n, p.status);
       cb[f] = ld(F.b + idx);
       cc[f] = ld(F.c + idx);
     }
@@ -219,8 +253,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
   if (SPECIAL && (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN)) {
     for (int s = 0; s < p.n_src; ++s) {
       if (k == p.src[s].plane) {
-        sa = ld(p.src[s].v0 + col);
-        sb = ld(p.src[s].v1 + col);
+        sa = ldg_c(p.src[s].v0, col, p.plane, p.status);
+        sb = ldg_c(p.src[s].v1, col, p.plane, p.status);
         on_src = true;
       }
     }
@@ -335,8 +369,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;
-    p.cpml[f].psi0[cli[f]] = cp0[f];
-    p.cpml[f].psi1[cli[f]] = cp1[f];
+    st_c(p.cpml[f].psi0, cli[f], p.cpml[f].n, p.status, cp0[f]);
+    st_c(p.cpml[f].psi1, cli[f], p.cpml[f].n, p.status, cp1[f]);
   }
 }
 
@@ -359,8 +393,8 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
       if (face_axis(f) == 2) cli[f] = ((k - F.lo) * p.ny + j) * p.nx + i;
       else if (face_axis(f) == 0) cli[f] = ((k - F.zlo) * p.ny + j) * F.ex + (i + 1 - F.lo);
       else cli[f] = ((k - F.zlo) * F.ey + (j + 1 - F.lo)) * p.nx + i;
-      cp0[f] = F.psi0[cli[f]];
-      cp1[f] = F.psi1[cli[f]];
+      cp0[f] = ld_c(F.psi0, cli[f], F.n, p.status);
+      cp1[f] = ld_c(F.psi1, cli[f], F.n, p.status);
       cb[f] = ld(F.b + idx);
       cc[f] = ld(F.c + idx);
     }
@@ -369,8 +403,8 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
   bool on_src = false;
   for (int s = 0; SPECIAL && s < p.n_src; ++s) {
     if (k == p.src[s].plane) {
-      sa = ld(p.src[s].v0 + col);
-      sb = ld(p.src[s].v1 + col);
+      sa = ldg_c(p.src[s].v0, col, p.plane, p.status);
+      sb = ldg_c(p.src[s].v1, col, p.plane, p.status);
       on_src = true;
     }
   }
@@ -405,8 +439,8 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;
-    p.cpml[f].psi0[cli[f]] = cp0[f];
-    p.cpml[f].psi1[cli[f]] = cp1[f];
+    st_c(p.cpml[f].psi0, cli[f], p.cpml[f].n, p.status, cp0[f]);
+    st_c(p.cpml[f].psi1, cli[f], p.cpml[f].n, p.status, cp1[f]);
   }
 }
 

@@ -24,7 +24,9 @@ enum Mode { MODE_PLAIN = 0, MODE_NL = 1, MODE_PLRC_LIN = 2, MODE_PLRC_NONLIN = 3
 enum Face { FACE_NORTH = 0, FACE_SOUTH, FACE_WEST, FACE_EAST, FACE_UP, FACE_DOWN };
 
 // Device status word, read back after mp_step.
-enum StatusSlot { ST_NEWTON = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_COUNT = 4 };
+// ST_BOUNDS counts the accesses a checked build (MPB_CHECKED=1) found outside
+// their array and skipped.
+enum StatusSlot { ST_NEWTON = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_BOUNDS = 3, ST_COUNT = 4 };
 
 // Tile of the TMA-staged kernels (mp_step_tma.cu): 32 x 8 columns.
 static const int kTmaTileX = 32, kTmaTileY = 8;
@@ -50,6 +52,7 @@ struct CpmlFace {
   int zlo;          // first z plane of the box (for x/y faces)
   int ex, ey;       // box extents in x and y (for the index)
   T *psi0, *psi1;   // psi components as in cpml_border.cpp:361-383 / :460-482
+  int n;            // elements of psi0 / psi1 (checked builds test indices against it)
   const T *b;       // b coefficient per index along dim (full axis length)
   const T *c;       // c / Delta per index along dim
 };
@@ -110,6 +113,8 @@ struct EParams {
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
   int *status;
+  long long n_field;      // elements of each field and history array
+  long long n_psi;        // pairs of each PLRC accumulator array
 };
 
 template <typename T>
@@ -129,6 +134,7 @@ struct BParams {
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
   int *status;
+  long long n_field;      // elements of each field array
 };
 
 // ---------------------------------------------------------------------------

@@ -108,25 +108,27 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
 
   int km = k0 - 1;
   if (p.zperiodic && km == 0) km = p.nz;
-  T bx_km = ld(Bx + km * plane + col);
-  T by_km = ld(By + km * plane + col);
+  const long long nf = p.n_field;
+  int *const st = p.status;
+  T bx_km = ldg_c(Bx, km * plane + col, nf, st);
+  T by_km = ldg_c(By, km * plane + col, nf, st);
 
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * plane;
     // ---- loads of this cell (the rest are in e_cell, still before any store)
     EIn<T> v;
-    v.bx = ld(Bx + base + col);
-    v.by = ld(By + base + col);
-    v.bz = ld(Bz + base + col);
-    v.bz_xm = ld(Bz + base + colxm);
-    v.by_xm = ld(By + base + colxm);
-    v.bz_ym = ld(Bz + base + colym);
-    v.bx_ym = ld(Bx + base + colym);
+    v.bx = ldg_c(Bx, base + col, nf, st);
+    v.by = ldg_c(By, base + col, nf, st);
+    v.bz = ldg_c(Bz, base + col, nf, st);
+    v.bz_xm = ldg_c(Bz, base + colxm, nf, st);
+    v.by_xm = ldg_c(By, base + colxm, nf, st);
+    v.bz_ym = ldg_c(Bz, base + colym, nf, st);
+    v.bx_ym = ldg_c(Bx, base + colym, nf, st);
     v.bx_km = bx_km;
     v.by_km = by_km;
-    v.ex = Ex[base + col];
-    v.ey = Ey[base + col];
-    v.ez = Ez[base + col];
+    v.ex = ld_c(Ex, base + col, nf, st);
+    v.ey = ld_c(Ey, base + col, nf, st);
+    v.ez = ld_c(Ez, base + col, nf, st);
     const T ikz = ld(p.ik[2] + k);
     const bool med = (MODE == MODE_PLRC_LIN || MODE == MODE_PLRC_NONLIN) && k >= p.mz0 && k <= p.mz1;
     const long long pi = ((long long)(k - p.mz0) * p.ny + j) * p.nx + i;
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
 #pragma unroll
       for (int n = 0; n < NP; ++n)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) q[n][c] = reinterpret_cast<const T2 *>(p.psi[n][c])[pi];
+        for (int c = 0; c < 3; ++c) q[n][c] = ld_c(reinterpret_cast<const T2 *>(p.psi[n][c]), pi, p.n_psi, st);
     }
     T exn, eyn, ezn;
     if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
@@ -143,19 +145,19 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
     else
       e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
     // ---- stores
-    Ex[base + col] = exn;
-    Ey[base + col] = eyn;
-    Ez[base + col] = ezn;
+    st_c(Ex, base + col, nf, st, exn);
+    st_c(Ey, base + col, nf, st, eyn);
+    st_c(Ez, base + col, nf, st, ezn);
     if (DESIGN && p.hist[0]) {
-      p.hist[0][base + col] = exn;
-      p.hist[1][base + col] = eyn;
-      p.hist[2][base + col] = ezn;
+      st_c(p.hist[0], base + col, nf, st, exn);
+      st_c(p.hist[1], base + col, nf, st, eyn);
+      st_c(p.hist[2], base + col, nf, st, ezn);
     }
     if (NP > 0 && med) {
 #pragma unroll
       for (int n = 0; n < NP; ++n)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) reinterpret_cast<T2 *>(p.psi[n][c])[pi] = q[n][c];
+        for (int c = 0; c < 3; ++c) st_c(reinterpret_cast<T2 *>(p.psi[n][c]), pi, p.n_psi, st, q[n][c]);
     }
     bx_km = v.bx;
     by_km = v.by;
@@ -192,6 +194,8 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
   const int2 srck = source_plane_range(p);
 
   // loads of plane k (ex, ey of plane k are carried from the previous plane)
+  const long long nf = p.n_field;
+  int *const st = p.status;
   auto load = [&](int k, T ex_k, T ey_k, BIn<T> &v) {
     const long long base = (long long)k * plane;
     int kp = k + 1;
@@ -199,20 +203,20 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
     const long long basep = (long long)kp * plane;
     v.ex = ex_k;
     v.ey = ey_k;
-    v.ex_kp = ld(Ex + basep + col);
-    v.ey_kp = ld(Ey + basep + col);
-    v.ez = ld(Ez + base + col);
-    v.ez_xp = ld(Ez + base + colxp);
-    v.ey_xp = ld(Ey + base + colxp);
-    v.ez_yp = ld(Ez + base + colyp);
-    v.ex_yp = ld(Ex + base + colyp);
-    v.bx = Bx[base + col];
-    v.by = By[base + col];
-    v.bz = Bz[base + col];
+    v.ex_kp = ldg_c(Ex, basep + col, nf, st);
+    v.ey_kp = ldg_c(Ey, basep + col, nf, st);
+    v.ez = ldg_c(Ez, base + col, nf, st);
+    v.ez_xp = ldg_c(Ez, base + colxp, nf, st);
+    v.ey_xp = ldg_c(Ey, base + colxp, nf, st);
+    v.ez_yp = ldg_c(Ez, base + colyp, nf, st);
+    v.ex_yp = ldg_c(Ex, base + colyp, nf, st);
+    v.bx = ld_c(Bx, base + col, nf, st);
+    v.by = ld_c(By, base + col, nf, st);
+    v.bz = ld_c(Bz, base + col, nf, st);
   };
 
   BIn<T> v;
-  load(k0, ld(Ex + (long long)k0 * plane + col), ld(Ey + (long long)k0 * plane + col), v);
+  load(k0, ldg_c(Ex, (long long)k0 * plane + col, nf, st), ldg_c(Ey, (long long)k0 * plane + col, nf, st), v);
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * plane;
 #if MPB_B_PREFETCH
@@ -227,9 +231,9 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y, MPB_B_MIN_THREADS / (32 * 
       b_cell<T, true>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
     else
       b_cell<T, false>(p, i, j, k, col, cmask, v, ikx, iky, iky_bz, ikz, bxn, byn, bzn);
-    Bx[base + col] = bxn;
-    By[base + col] = byn;
-    Bz[base + col] = bzn;
+    st_c(Bx, base + col, nf, st, bxn);
+    st_c(By, base + col, nf, st, byn);
+    st_c(Bz, base + col, nf, st, bzn);
 #if MPB_B_PREFETCH
     v = vn;
 #else
@@ -280,6 +284,29 @@ __device__ __forceinline__ void stv(T *p, const RowV<T> &r) {
   *reinterpret_cast<VT *>(p) = x;
 }
 
+// The vector accesses at element i of an array of n elements, checked like
+// ldg_c / ld_c / st_c (both elements must lie inside).
+template <typename T>
+__device__ __forceinline__ RowV<T> ldv_c(const T *a, long long i, long long n, int *status) {
+  if (in_bounds(i + kBV - 1, n, status) && in_bounds(i, n, status)) return ldv(a + i);
+  RowV<T> r;
+#pragma unroll
+  for (int c = 0; c < kBV; ++c) r.v[c] = T(0);
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ RowV<T> ldv_rw_c(const T *a, long long i, long long n, int *status) {
+  if (in_bounds(i + kBV - 1, n, status) && in_bounds(i, n, status)) return ldv_rw(a + i);
+  RowV<T> r;
+#pragma unroll
+  for (int c = 0; c < kBV; ++c) r.v[c] = T(0);
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stv_c(T *a, long long i, long long n, int *status, const RowV<T> &r) {
+  if (in_bounds(i + kBV - 1, n, status) && in_bounds(i, n, status)) stv(a + i, r);
+}
+
 // psi_H of the face in slot F at one cell (cpml_border.cpp:499-527): updates
 // the layer arrays and adds the face's currents to m (MPulse's order: slots
 // in turn, as b_cell sums them).  d0 / d1: the differences of E along the
@@ -294,10 +321,10 @@ __device__ __forceinline__ void b_face(const BParams<T> &p, int i, int j, int k,
   else if (dim == 0) li = ((k - L.zlo) * p.ny + j) * L.ex + (i + 1 - L.lo);
   else li = ((k - L.zlo) * L.ey + (j + 1 - L.lo)) * p.nx + i;
   const T b = ld(L.b + idx), c = ld(L.c + idx);
-  const T c0 = b * L.psi0[li] + c * d0;
-  const T c1 = b * L.psi1[li] + c * d1;
-  L.psi0[li] = c0;
-  L.psi1[li] = c1;
+  const T c0 = b * ld_c(L.psi0, li, L.n, p.status) + c * d0;
+  const T c1 = b * ld_c(L.psi1, li, L.n, p.status) + c * d1;
+  st_c(L.psi0, li, L.n, p.status, c0);
+  st_c(L.psi1, li, L.n, p.status, c1);
   if (dim == 2) { m[0] += c0; m[1] += c1; }
   else if (dim == 0) { m[1] += c0; m[2] += c1; }
   else { m[2] += c0; m[0] += c1; }
@@ -340,18 +367,21 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
   for (int c = 0; c < V; ++c) xbits |= ((face_column_mask(p.cpml, i0 + c, j) >> 2) & 3u) << (2 * c);
   const int2 srck = source_plane_range(p);
 
-  RowV<T> ex = ldv(Ex + (long long)k0 * plane + col), ey = ldv(Ey + (long long)k0 * plane + col);
+  const long long nf = p.n_field;
+  int *const st = p.status;
+  RowV<T> ex = ldv_c(Ex, (long long)k0 * plane + col, nf, st), ey = ldv_c(Ey, (long long)k0 * plane + col, nf, st);
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * plane;
     int kp = k + 1;
     if (p.zperiodic && kp == p.nz + 1) kp = 1;
     const long long basep = (long long)kp * plane;
     // ---- every load of this plane first
-    const RowV<T> ex_kp = ldv(Ex + basep + col), ey_kp = ldv(Ey + basep + col);
-    const RowV<T> ez = ldv(Ez + base + col);
-    const T ez_xl = ld(Ez + base + colxl), ey_xl = ld(Ey + base + colxl);
-    const RowV<T> ez_yp = ldv(Ez + base + colyp), ex_yp = ldv(Ex + base + colyp);
-    const RowV<T> bx = ldv_rw(Bx + base + col), by = ldv_rw(By + base + col), bz = ldv_rw(Bz + base + col);
+    const RowV<T> ex_kp = ldv_c(Ex, basep + col, nf, st), ey_kp = ldv_c(Ey, basep + col, nf, st);
+    const RowV<T> ez = ldv_c(Ez, base + col, nf, st);
+    const T ez_xl = ldg_c(Ez, base + colxl, nf, st), ey_xl = ldg_c(Ey, base + colxl, nf, st);
+    const RowV<T> ez_yp = ldv_c(Ez, base + colyp, nf, st), ex_yp = ldv_c(Ex, base + colyp, nf, st);
+    const RowV<T> bx = ldv_rw_c(Bx, base + col, nf, st), by = ldv_rw_c(By, base + col, nf, st),
+                  bz = ldv_rw_c(Bz, base + col, nf, st);
     const T ikz = ld(p.ik[2] + k);
     // ---- H-side currents, in MPulse's order: faces by slot, then the injector
     T m[V][3];
@@ -390,7 +420,7 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
         if (k != p.src[s].plane) continue;
 #pragma unroll
         for (int c = 0; c < V; ++c) {
-          const T sa = ld(p.src[s].v0 + col + c), sb = ld(p.src[s].v1 + col + c);
+          const T sa = ldg_c(p.src[s].v0, col + c, p.plane, st), sb = ldg_c(p.src[s].v1, col + c, p.plane, st);
           for (int q = 0; q < p.src_mult; ++q) {
             m[c][0] += sa;
             m[c][1] += sb;
@@ -409,9 +439,9 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
       byn.v[c] = by.v[c] + dt * ((ezx - ez.v[c]) * ikx[c] - (ex_kp.v[c] - ex.v[c]) * ikz + m[c][1]);
       bzn.v[c] = bz.v[c] + dt * ((ex_yp.v[c] - ex.v[c]) * iky_bz - (eyx - ey.v[c]) * ikx[c] + m[c][2]);
     }
-    stv(Bx + base + col, bxn);
-    stv(By + base + col, byn);
-    stv(Bz + base + col, bzn);
+    stv_c(Bx, base + col, nf, st, bxn);
+    stv_c(By, base + col, nf, st, byn);
+    stv_c(Bz, base + col, nf, st, bzn);
     ex = ex_kp;
     ey = ey_kp;
   }

@@ -23,6 +23,7 @@
 // The Kerr linearisation and the gradient accumulation are FP64; the rest is
 // in the precision of the forward state.  Memory-bound; one thread per (x, y)
 // column and chunk of planes.
+#include "mp_checked.cuh"
 #include "mp_device.h"
 
 #include <cuda_runtime.h>
@@ -84,10 +85,10 @@ __device__ __forceinline__ R comp1(const R v[3]) {
 
 // c * total at element li of an entry, or zero for pos < 0
 template <typename T, typename R>
-__device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, int li, R c, R &w0, R &w1) {
+__device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, int li, R c, R &w0, R &w1, int *st) {
   if (pos >= 0) {
-    w0 = c * R(F.a0[li]);
-    w1 = c * R(F.a1[li]);
+    w0 = c * R(ld_c(F.a0, li, F.n, st));
+    w1 = c * R(ld_c(F.a1, li, F.n, st));
   } else {
     w0 = w1 = R(0);
   }
@@ -114,6 +115,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   const long long pl = p.plane;
   const int col = j * nx + i, colxm = j * nx + im, colym = jm * nx + i;
   const R dt = R(p.dt);
+  const long long nf = p.n_field;
+  int *const st = p.status;
   const R kxi = p.ikH[0][i + 1], kxm = p.ikH[0][im + 1];
   const R kyj = p.ikH[1][j + 1], kym = p.ikH[1][jm + 1];
   const R bzj = p.ikH_bzy[j + 1], bzm = p.ikH_bzy[jm + 1];
@@ -132,13 +135,13 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   {
     const int pz = face_pos(HZ, k0 - 1);
     cw_on = pz >= 0;
-    face_w(HZ, pz, pz * plane + col, pz >= 0 ? R(HZ.c[k0 - 1]) : R(0), cw0, cw1);
+    face_w(HZ, pz, pz * plane + col, pz >= 0 ? R(HZ.c[k0 - 1]) : R(0), cw0, cw1, st);
   }
   const DesignParams &d = p.design;
   const bool dxy = i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1;
   const bool oxy = i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
-  R bx_km = Bx[(long long)(k0 - 1) * pl + col];
-  R by_km = By[(long long)(k0 - 1) * pl + col];
+  R bx_km = ld_c(Bx, (long long)(k0 - 1) * pl + col, nf, st);
+  R by_km = ld_c(By, (long long)(k0 - 1) * pl + col, nf, st);
 
   const bool plrc_nl = p.nonlin != 0;
   for (int k = k0; k <= k1; ++k) {
@@ -147,15 +150,16 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     const bool med = k >= p.mz0 && k <= p.mz1;
     const bool dcell = med && dxy && k >= d.z0 && k <= d.z1;
     // ---- every load of this plane first, so that their latencies overlap
-    const R bx = Bx[c0], by = By[c0], bz = Bz[c0];
-    const R bx_ym = Bx[base + colym], by_xm = By[base + colxm], bz_ym = Bz[base + colym], bz_xm = Bz[base + colxm];
+    const R bx = ld_c(Bx, c0, nf, st), by = ld_c(By, c0, nf, st), bz = ld_c(Bz, c0, nf, st);
+    const R bx_ym = ld_c(Bx, base + colym, nf, st), by_xm = ld_c(By, base + colxm, nf, st),
+            bz_ym = ld_c(Bz, base + colym, nf, st), bz_xm = ld_c(Bz, base + colxm, nf, st);
     const R kzk = p.ikH[2][k], kzm = p.ikH[2][k - 1];
-    R a[3] = {R(p.Eb[0][c0]), R(p.Eb[1][c0]), R(p.Eb[2][c0])};
-    const R En[3] = {R(p.En[0][c0]), R(p.En[1][c0]), R(p.En[2][c0])};
+    R a[3] = {R(ld_c(p.Eb[0], c0, nf, st)), R(ld_c(p.Eb[1], c0, nf, st)), R(ld_c(p.Eb[2], c0, nf, st))};
+    const R En[3] = {R(ld_c(p.En[0], c0, nf, st)), R(ld_c(p.En[1], c0, nf, st)), R(ld_c(p.En[2], c0, nf, st))};
     R En1[3] = {R(0), R(0), R(0)};
     if (med && (plrc_nl || dcell)) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) En1[c] = R(p.En1[c][c0]);
+      for (int c = 0; c < 3; ++c) En1[c] = R(ld_c(p.En1[c], c0, nf, st));
     }
     const long long pi = ((long long)(k - p.mz0) * ny + j) * nx + i;
     R pq[NP > 0 ? NP : 1][3][2];
@@ -164,17 +168,17 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       for (int n = 0; n < NP; ++n)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          pq[n][c][0] = p.psib[n][c][2 * pi];
-          pq[n][c][1] = p.psib[n][c][2 * pi + 1];
+          pq[n][c][0] = ld_c(p.psib[n][c], 2 * pi, 2 * p.n_psi, st);
+          pq[n][c][1] = ld_c(p.psib[n][c], 2 * pi + 1, 2 * p.n_psi, st);
         }
     }
     long long di = 0;
     double e = p.eps, s = 1.0, u = 1.0;
     if (dcell) {
       di = ((long long)(k - d.z0) * d.by + (j - d.y0)) * d.bx + (i - d.x0);
-      e = d.eps[di];
-      s = d.dscale[di];
-      u = d.chiscale[di];
+      e = ld_c(d.eps, di, p.n_design, st);
+      s = ld_c(d.dscale, di, p.n_design, st);
+      u = ld_c(d.chiscale, di, p.n_design, st);
     }
     // H-face totals (x, y at this column and x-1 / y-1; z at this plane) and
     // E-face totals of this cell, on warps and planes that touch a face
@@ -194,22 +198,22 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       const int chyo = face_col<1>(HY, hyo, i, j, nx), chym = face_col<1>(HY, hym, i, jm, nx);
       const int cexo = face_col<0>(EX, exo, i, j, nx), ceyo = face_col<1>(EY, eyo, i, j, nx);
       const int shx = face_plane<0>(HX, k, nx, ny), shy = face_plane<1>(HY, k, nx, ny);
-      face_w(HX, hxo, chxo + shx, hxco, hx0o, hx1o);
-      face_w(HX, hxm, chxm + shx, hxcm, hx0m, hx1m);
-      face_w(HY, hyo, chyo + shy, hyco, hy0o, hy1o);
-      face_w(HY, hym, chym + shy, hycm, hy0m, hy1m);
-      face_w(HZ, hzp, hzp * plane + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1);
+      face_w(HX, hxo, chxo + shx, hxco, hx0o, hx1o, st);
+      face_w(HX, hxm, chxm + shx, hxcm, hx0m, hx1m, st);
+      face_w(HY, hyo, chyo + shy, hyco, hy0o, hy1o, st);
+      face_w(HY, hym, chym + shy, hycm, hy0m, hy1m, st);
+      face_w(HZ, hzp, hzp * plane + col, hzp >= 0 ? R(HZ.c[k]) : R(0), hz0, hz1, st);
       lexo = exo >= 0 ? cexo + face_plane<0>(EX, k, nx, ny) : -1;
       leyo = eyo >= 0 ? ceyo + face_plane<1>(EY, k, nx, ny) : -1;
       lezo = ezp * plane + col;
-      if (lexo >= 0) { ex0 = EX.a0[lexo]; ex1 = EX.a1[lexo]; }
-      if (leyo >= 0) { ey0 = EY.a0[leyo]; ey1 = EY.a1[leyo]; }
-      if (ezp >= 0) { ez0 = EZ.a0[lezo]; ez1 = EZ.a1[lezo]; ezb = EZ.b[k]; }
+      if (lexo >= 0) { ex0 = ld_c(EX.a0, lexo, EX.n, st); ex1 = ld_c(EX.a1, lexo, EX.n, st); }
+      if (leyo >= 0) { ey0 = ld_c(EY.a0, leyo, EY.n, st); ey1 = ld_c(EY.a1, leyo, EY.n, st); }
+      if (ezp >= 0) { ez0 = ld_c(EZ.a0, lezo, EZ.n, st); ez1 = ld_c(EZ.a1, lezo, EZ.n, st); ezb = EZ.b[k]; }
     }
     R obx = R(0), oby = R(0);
     if (p.add_obj && oxy && p.obj_kind == 2 && k == p.oz0) {
-      obx = p.obx[col];
-      oby = p.oby[col];
+      obx = ld_c(p.obx, col, pl, st);
+      oby = ld_c(p.oby, col, pl, st);
     }
 
     // ---- adjoint of E' (B half transposed)
@@ -324,9 +328,9 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
 #pragma unroll
           for (int c = 0; c < 3; ++c) gu += (double)g[c] * p.chi * (double)E2 * (double)En[c];
         }
-        p.grad[0][di] += ge;
-        p.grad[1][di] += gs;
-        p.grad[2][di] += gu;
+        st_c(p.grad[0], di, p.n_design, st, ld_c(p.grad[0], di, p.n_design, st) + ge);
+        st_c(p.grad[1], di, p.n_design, st, ld_c(p.grad[1], di, p.n_design, st) + gs);
+        st_c(p.grad[2], di, p.n_design, st, ld_c(p.grad[2], di, p.n_design, st) + gu);
       }
     }
     // the objective's E term of the state before the step
@@ -345,33 +349,33 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     // ---- stores
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      p.G[c][c0] = T(g[c]);
-      p.Eb[c][c0] = T(ne[c]);
+      st_c(p.G[c], c0, nf, st, T(g[c]));
+      st_c(p.Eb[c], c0, nf, st, T(ne[c]));
     }
     if (med) {
 #pragma unroll
       for (int n = 0; n < NP; ++n)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          p.psib[n][c][2 * pi] = T(pq[n][c][0]);
-          p.psib[n][c][2 * pi + 1] = T(pq[n][c][1]);
+          st_c(p.psib[n][c], 2 * pi, 2 * p.n_psi, st, T(pq[n][c][0]));
+          st_c(p.psib[n][c], 2 * pi + 1, 2 * p.n_psi, st, T(pq[n][c][1]));
         }
     }
     // E-face totals of this cell: b * total + dt * G
     if (fpl) {
       if (lexo >= 0) {
         const R exb = R(EX.b[i + 1]);
-        EX.a0[lexo] = T(exb * ex0 + dt * comp0<0>(g));
-        EX.a1[lexo] = T(exb * ex1 + dt * comp1<0>(g));
+        st_c(EX.a0, lexo, EX.n, st, T(exb * ex0 + dt * comp0<0>(g)));
+        st_c(EX.a1, lexo, EX.n, st, T(exb * ex1 + dt * comp1<0>(g)));
       }
       if (leyo >= 0) {
         const R eyb = R(EY.b[j + 1]);
-        EY.a0[leyo] = T(eyb * ey0 + dt * comp0<1>(g));
-        EY.a1[leyo] = T(eyb * ey1 + dt * comp1<1>(g));
+        st_c(EY.a0, leyo, EY.n, st, T(eyb * ey0 + dt * comp0<1>(g)));
+        st_c(EY.a1, leyo, EY.n, st, T(eyb * ey1 + dt * comp1<1>(g)));
       }
       if (ezp >= 0) {
-        EZ.a0[lezo] = T(ezb * ez0 + dt * comp0<2>(g));
-        EZ.a1[lezo] = T(ezb * ez1 + dt * comp1<2>(g));
+        st_c(EZ.a0, lezo, EZ.n, st, T(ezb * ez0 + dt * comp0<2>(g)));
+        st_c(EZ.a1, lezo, EZ.n, st, T(ezb * ez1 + dt * comp1<2>(g)));
       }
     }
     bx_km = bx;
@@ -395,6 +399,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
   const long long pl = p.plane;
   const int col = j * nx + i, colxp = j * nx + ip, colyp = jp * nx + i;
   const R dt = R(p.dt);
+  const long long nf = p.n_field;
+  int *const st = p.status;
   const R kxi = p.ikE[0][i + 1], kxp = p.ikE[0][ip + 1];
   const R kyj = p.ikE[1][j + 1], kyp = p.ikE[1][jp + 1];
   const T *gx = p.G[0], *gy = p.G[1], *gz = p.G[2];
@@ -417,24 +423,25 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
   const bool warp_xy =
       __any_sync(__activemask(), (exo >= 0) || (exp_ >= 0) || (eyo >= 0) || (eyp >= 0) || (hxo >= 0) || (hyo >= 0));
   // G and the z E face's c * total at plane k, carried from the previous plane's k + 1
-  R gx_k = gx[(long long)k0 * pl + col], gy_k = gy[(long long)k0 * pl + col];
+  R gx_k = ld_c(gx, (long long)k0 * pl + col, nf, st), gy_k = ld_c(gy, (long long)k0 * pl + col, nf, st);
   R zw0, zw1;
   bool zw_on;
   {
     const int pz = face_pos(EZ, k0);
     zw_on = pz >= 0;
-    face_w(EZ, pz, pz * plane + col, pz >= 0 ? R(EZ.c[k0]) : R(0), zw0, zw1);
+    face_w(EZ, pz, pz * plane + col, pz >= 0 ? R(EZ.c[k0]) : R(0), zw0, zw1, st);
   }
 
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * pl;
     const long long c0 = base + col;
     // ---- every load of this plane first
-    const R gx_kp = gx[c0 + pl], gy_kp = gy[c0 + pl];
-    const R gzk = gz[c0];
-    const R gx_yp = gx[base + colyp], gy_xp = gy[base + colxp], gz_xp = gz[base + colxp], gz_yp = gz[base + colyp];
+    const R gx_kp = ld_c(gx, c0 + pl, nf, st), gy_kp = ld_c(gy, c0 + pl, nf, st);
+    const R gzk = ld_c(gz, c0, nf, st);
+    const R gx_yp = ld_c(gx, base + colyp, nf, st), gy_xp = ld_c(gy, base + colxp, nf, st),
+            gz_xp = ld_c(gz, base + colxp, nf, st), gz_yp = ld_c(gz, base + colyp, nf, st);
     const R kzk = p.ikE[2][k], kzp = p.ikE[2][k + 1];
-    R b[3] = {R(p.Bb[0][c0]), R(p.Bb[1][c0]), R(p.Bb[2][c0])};
+    R b[3] = {R(ld_c(p.Bb[0], c0, nf, st)), R(ld_c(p.Bb[1], c0, nf, st)), R(ld_c(p.Bb[2], c0, nf, st))};
     // faces on warps and planes that touch one: E faces (x / y hold planes
     // 1..nz; z at plane k + 1, plane k carried) and the H-face totals of this cell
     const int ezq = face_pos(EZ, k + 1), hzp = face_pos(HZ, k);
@@ -447,24 +454,24 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     if (fpl) {
       if (k >= 1) {
         const int sex = face_plane<0>(EX, k, nx, ny), sey = face_plane<1>(EY, k, nx, ny);
-        face_w(EX, exo, cexo + sex, exco, ex0o, ex1o);
-        face_w(EX, exp_, cexp + sex, excp, ex0p, ex1p);
-        face_w(EY, eyo, ceyo + sey, eyco, ey0o, ey1o);
-        face_w(EY, eyp, ceyp + sey, eycp, ey0p, ey1p);
+        face_w(EX, exo, cexo + sex, exco, ex0o, ex1o, st);
+        face_w(EX, exp_, cexp + sex, excp, ex0p, ex1p, st);
+        face_w(EY, eyo, ceyo + sey, eyco, ey0o, ey1o, st);
+        face_w(EY, eyp, ceyp + sey, eycp, ey0p, ey1p, st);
       }
-      face_w(EZ, ezq, ezq * plane + col, ezq >= 0 ? R(EZ.c[k + 1]) : R(0), ez0p, ez1p);
+      face_w(EZ, ezq, ezq * plane + col, ezq >= 0 ? R(EZ.c[k + 1]) : R(0), ez0p, ez1p, st);
       lhx = chxo + face_plane<0>(HX, k, nx, ny);
       lhy = chyo + face_plane<1>(HY, k, nx, ny);
       lhz = hzp * plane + col;
-      if (hxk) { hx0 = HX.a0[lhx]; hx1 = HX.a1[lhx]; }
-      if (hyk) { hy0 = HY.a0[lhy]; hy1 = HY.a1[lhy]; }
-      if (hzp >= 0) { hz0 = HZ.a0[lhz]; hz1 = HZ.a1[lhz]; hzb = HZ.b[k]; }
+      if (hxk) { hx0 = ld_c(HX.a0, lhx, HX.n, st); hx1 = ld_c(HX.a1, lhx, HX.n, st); }
+      if (hyk) { hy0 = ld_c(HY.a0, lhy, HY.n, st); hy1 = ld_c(HY.a1, lhy, HY.n, st); }
+      if (hzp >= 0) { hz0 = ld_c(HZ.a0, lhz, HZ.n, st); hz1 = ld_c(HZ.a1, lhz, HZ.n, st); hzb = HZ.b[k]; }
     }
     const bool obj = oxy && k == p.oz0;
     R oex = R(0), oey = R(0);
     if (obj) {
-      oex = p.En[0][c0];
-      oey = p.En[1][c0];
+      oex = ld_c(p.En[0], c0, nf, st);
+      oey = ld_c(p.En[1], c0, nf, st);
     }
 
     // ---- transposed curl_E and E faces
@@ -498,19 +505,19 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
 
     // ---- stores: B adjoint, H-face totals for the step before (b * total + dt * B adjoint)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) p.Bb[c][c0] = T(b[c]);
+    for (int c = 0; c < 3; ++c) st_c(p.Bb[c], c0, nf, st, T(b[c]));
     if (fpl) {
       if (hxk) {
-        HX.a0[lhx] = T(hxb * hx0 + dt * comp0<0>(b));
-        HX.a1[lhx] = T(hxb * hx1 + dt * comp1<0>(b));
+        st_c(HX.a0, lhx, HX.n, st, T(hxb * hx0 + dt * comp0<0>(b)));
+        st_c(HX.a1, lhx, HX.n, st, T(hxb * hx1 + dt * comp1<0>(b)));
       }
       if (hyk) {
-        HY.a0[lhy] = T(hyb * hy0 + dt * comp0<1>(b));
-        HY.a1[lhy] = T(hyb * hy1 + dt * comp1<1>(b));
+        st_c(HY.a0, lhy, HY.n, st, T(hyb * hy0 + dt * comp0<1>(b)));
+        st_c(HY.a1, lhy, HY.n, st, T(hyb * hy1 + dt * comp1<1>(b)));
       }
       if (hzp >= 0) {
-        HZ.a0[lhz] = T(hzb * hz0 + dt * comp0<2>(b));
-        HZ.a1[lhz] = T(hzb * hz1 + dt * comp1<2>(b));
+        st_c(HZ.a0, lhz, HZ.n, st, T(hzb * hz0 + dt * comp0<2>(b)));
+        st_c(HZ.a1, lhz, HZ.n, st, T(hzb * hz1 + dt * comp1<2>(b)));
       }
     }
     gx_k = gx_kp;
@@ -528,37 +535,39 @@ __global__ void __launch_bounds__(256) adj_init_kernel(const AdjParams<T> p) {
   const int k = blockIdx.z;  // 0..nz
   if (i >= p.nx || j >= p.ny) return;
   const long long col = (long long)j * p.nx + i, c0 = (long long)k * p.plane + col;
+  const long long nf = p.n_field;
+  int *const st = p.status;
   double e[3] = {0.0, 0.0, 0.0}, b[3] = {0.0, 0.0, 0.0};
   const bool inxy = i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
   if (p.obj_kind == 1) {
     if (inxy && k >= p.oz0 && k <= p.oz1)
-      for (int c = 0; c < 3; ++c) e[c] = p.obj_f * (double)p.En[c][c0];
+      for (int c = 0; c < 3; ++c) e[c] = p.obj_f * (double)ld_c(p.En[c], c0, nf, st);
   } else if (inxy && k == p.oz0) {
-    e[0] = p.obj_f * (double)p.oby[col];
-    e[1] = -p.obj_f * (double)p.obx[col];
-    b[0] = -p.obj_f * (double)p.En[1][c0];
-    b[1] = p.obj_f * (double)p.En[0][c0];
+    e[0] = p.obj_f * (double)ld_c(p.oby, col, p.plane, st);
+    e[1] = -p.obj_f * (double)ld_c(p.obx, col, p.plane, st);
+    b[0] = -p.obj_f * (double)ld_c(p.En[1], c0, nf, st);
+    b[1] = p.obj_f * (double)ld_c(p.En[0], c0, nf, st);
   }
   for (int c = 0; c < 3; ++c) {
-    p.Eb[c][c0] = T(e[c]);
-    p.Bb[c][c0] = T(b[c]);
+    st_c(p.Eb[c], c0, nf, st, T(e[c]));
+    st_c(p.Bb[c], c0, nf, st, T(b[c]));
   }
   // H-face totals: dt times the adjoint of B
   const int hxo = face_pos(p.fh[0], i + 1), hyo = face_pos(p.fh[1], j + 1), hzo = face_pos(p.fh[2], k);
   if (hxo >= 0 && k >= p.fh[0].zlo) {
     const int li = face_col<0>(p.fh[0], hxo, i, j, p.nx) + face_plane<0>(p.fh[0], k, p.nx, p.ny);
-    p.fh[0].a0[li] = T(p.dt * comp0<0>(b));
-    p.fh[0].a1[li] = T(p.dt * comp1<0>(b));
+    st_c(p.fh[0].a0, li, p.fh[0].n, st, T(p.dt * comp0<0>(b)));
+    st_c(p.fh[0].a1, li, p.fh[0].n, st, T(p.dt * comp1<0>(b)));
   }
   if (hyo >= 0 && k >= p.fh[1].zlo) {
     const int li = face_col<1>(p.fh[1], hyo, i, j, p.nx) + face_plane<1>(p.fh[1], k, p.nx, p.ny);
-    p.fh[1].a0[li] = T(p.dt * comp0<1>(b));
-    p.fh[1].a1[li] = T(p.dt * comp1<1>(b));
+    st_c(p.fh[1].a0, li, p.fh[1].n, st, T(p.dt * comp0<1>(b)));
+    st_c(p.fh[1].a1, li, p.fh[1].n, st, T(p.dt * comp1<1>(b)));
   }
   if (hzo >= 0) {
     const long long li = (long long)hzo * p.plane + col;
-    p.fh[2].a0[li] = T(p.dt * comp0<2>(b));
-    p.fh[2].a1[li] = T(p.dt * comp1<2>(b));
+    st_c(p.fh[2].a0, li, p.fh[2].n, st, T(p.dt * comp0<2>(b)));
+    st_c(p.fh[2].a1, li, p.fh[2].n, st, T(p.dt * comp1<2>(b)));
   }
 }
 

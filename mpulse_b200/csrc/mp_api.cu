@@ -1374,6 +1374,7 @@ int adj_faces(mp_ctx *c, DevBufs &buf, bool isH, const CpmlFace<T> *fw, AdjFace<
       return cuda_err(c, e, "adjoint allocation");
     F.a0 = static_cast<T *>(a0);
     F.a1 = static_cast<T *>(a1);
+    F.n = (long long)cells;
     if (!B) {
       F.b = fw[fa].b;
       F.c = fw[fa].c;
@@ -1662,6 +1663,10 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     if (rc != MP_OK) return rc;
   }
   p.nx = g.nx; p.ny = g.ny; p.nz = g.nz;
+  p.status = c->d_status;
+  p.n_field = (long long)c->fcount;
+  p.n_psi = (long long)c->psi_cells;
+  p.n_design = (long long)c->dcells;
   {
     // planes per block: enough blocks to fill 148 SMs several times over
     const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);

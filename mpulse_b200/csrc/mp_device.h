@@ -152,6 +152,7 @@ template <typename T>
 struct AdjFace {
   int active, lo0, hi0, lo1, hi1, n0, zlo, ex, ey;
   T *a0, *a1;
+  long long n;     // elements of a0 / a1
   const T *b, *c;  // b and c / Delta along the axis (full axis length, both faces)
 };
 
@@ -183,6 +184,8 @@ struct AdjParams {
   int ox0, ox1, oy0, oy1, oz0, oz1;  // 0-based x/y, MPulse z
   double obj_f;           // 2 dt (E^2 box) or dt dx dy (Sz plane)
   const T *obx, *oby;     // Bx, By of that state on the Sz plane (plane-sized)
+  int *status;            // the context's status word
+  long long n_field, n_psi, n_design;  // elements of a field array, pairs of a PLRC array, design cells
 };
 
 // Field initialisers (mp_init_kernels.cu).

@@ -93,6 +93,13 @@ CASES = {
                                          src_d=6, src=dict(t_size=40, t_off=0, length=0.2, width=0.1,
                                                            k0=2 * math.pi / 0.7, time=0.2, shift=-0.03,
                                                            amp=1.1, eps=1.2)),
+    # x a multiple of 64: the B half runs its two-cell vector kernel; with
+    # CPML on all faces its x-face (per cell), y-face (per row) and z-face
+    # paths, and the injection plane, all run
+    "vec_nonlin_all_short": dict(solver=P.MP_SOLVER_PLRC_NONLIN, n=(64, 12, 22), cpml=P.MP_CPML_ALL, cpml_d=4,
+                                 chi=0.2, medium=(8, 40), eps_bg=1.2, sources=(P.MP_SOURCE_SHORT_PULSE,), src_d=6),
+    "vec_lin_all_thick_wave": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(128, 9, 13), cpml=P.MP_CPML_ALL, cpml_d=5,
+                                   sources=(P.MP_SOURCE_PLANE_WAVE,), src_d=4),
     # x a multiple of 32 and y of 8: these run the TMA-staged kernels
     "tma_nonlin_all_short": dict(solver=P.MP_SOLVER_PLRC_NONLIN, n=(32, 16, 20), cpml=P.MP_CPML_ALL, cpml_d=4,
                                  chi=0.2, medium=(6, 30), sources=(P.MP_SOURCE_SHORT_PULSE,), src_d=5),

@@ -78,3 +78,33 @@ def test_tma_staging_needs_tile_multiples():
     cfg.staging = abi.MP_STAGING_TMA
     rc, msg = _create_error(cfg)
     assert rc == abi.MP_ERR_UNSUPPORTED and "multiple of 32" in msg
+
+
+def header_constants():
+    """NAME = value enumerators and #define NAME value constants of the header."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(MP_[A-Z0-9_]+)\s*=\s*(-?\d+)", text)}
+    out.update({m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(MP_[A-Z0-9_]+)\s+(-?\d+)", text)})
+    return out
+
+
+def test_header_constants_match_python_mirror():
+    consts = header_constants()
+    assert "MP_ERR_BOUNDS" in consts and "MP_SOLVER_PLRC_NONLIN" in consts
+    for name, value in consts.items():
+        if hasattr(abi, name):
+            assert getattr(abi, name) == value, name
+    # every status code has a name in the Python mirror
+    for name, value in consts.items():
+        if name.startswith("MP_ERR_") or name == "MP_OK":
+            assert getattr(abi, name) == value, name
+
+
+def test_checked_library_exports_the_same_symbols():
+    """libmpulse_b200_checked.so (MPB_CHECKED=1) is the same ABI."""
+    from mpulse_b200 import build
+    assert os.path.exists(build.LIB_CHECKED), "build the checked library: python -m mpulse_b200.build --checked"
+    L = C.CDLL(build.LIB_CHECKED)
+    for n in declared_functions():
+        assert hasattr(L, n), n

@@ -254,6 +254,7 @@ def run_ours(args) -> dict:
     # end to end through the C ABI with host buffers
     e2e = run_e2e(args, torch, stream, local_rank)
     adjoint = run_adjoint(local_rank) if rank == 0 else None
+    others = run_other_configs(local_rank, torch, stream) if rank == 0 else None
 
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -271,6 +272,7 @@ def run_ours(args) -> dict:
                       "max_abs_diff": float(np.max(np.abs(np.array(trace32) - np.array(trace64))))},
         "adjoint_forward_ratio": adjoint["fp32"]["ratio"] if adjoint else None,
         "adjoint": adjoint,
+        "other_workloads": others,
         "roofline": roofline, "step_roofline": step_roofline,
         "kernel_ms": kt,
         "e2e": e2e,
@@ -283,6 +285,59 @@ def run_ours(args) -> dict:
         dist.barrier()
         dist.destroy_process_group()
     return out if rank == 0 else None
+
+
+def run_other_configs(local_rank: int, torch, stream) -> dict:
+    """The parity workloads beside the headline one, FP32 and FP64 forms
+    (device time of the step loop, CUDA events): the 64^3 vacuum pulse
+    (pulse_init start, 400 steps) and the 128^3 linear PLRC workload
+    (plane_gauss_inject, 1000 steps).  The FP32 error of E against the FP64
+    form is taken every 100 steps of a second, untimed pair of runs: relative
+    L2 at the end and when the FP64 field norm peaks, and the final error over
+    that peak norm (late in these runs the pulse has left through the CPML
+    and the field that remains is small, so the final relative error alone
+    measures residue)."""
+    from mpulse_b200 import runtime
+    out = {}
+    for name, make, steps, init in (
+            ("c1_vacuum_pulse_64^3_400steps", configs.c1_vacuum_pulse, 400, configs.c1_initial_fields),
+            ("c2_linear_plrc_128^3_1000steps", configs.c2_linear_plrc, 1000, None)):
+        res, sims = {}, {}
+        for prec, tag in ((abi.MP_FP32, "fp32"), (abi.MP_FP64, "fp64")):
+            cfg = make(prec)
+            cfg.device = local_rank
+            with runtime.Simulation(cfg) as g:
+                g.set_stream(stream.cuda_stream)
+                if init is not None:
+                    for n, v in init(cfg).items():
+                        g.upload(n, v)
+                g.step(1)  # first launches out of the timed region
+                dt, _ = time_steps(g, torch, steps - 1, stream)
+            res[tag] = round(cfg.nx * cfg.ny * cfg.nz * (steps - 1) / dt / 1e9, 3)
+            sims[tag] = runtime.Simulation(cfg)
+            if init is not None:
+                for n, v in init(cfg).items():
+                    sims[tag].upload(n, v)
+        at_peak, peak, diff, norm = None, 0.0, 0.0, 0.0
+        for _ in range(steps // 100):
+            for g in sims.values():
+                g.step(100)
+            e32 = [sims["fp32"].download(n) for n in ("Ex", "Ey", "Ez")]
+            e64 = [sims["fp64"].download(n) for n in ("Ex", "Ey", "Ez")]
+            diff = math.sqrt(sum(float(np.sum((a - b) ** 2)) for a, b in zip(e32, e64)))
+            norm = math.sqrt(sum(float(np.sum(b ** 2)) for b in e64))
+            if norm > peak:
+                peak = norm
+                at_peak = diff / norm
+        for g in sims.values():
+            g.close()
+        res["unit"] = UNIT
+        res["rel_l2_fp32_vs_fp64_final"] = diff / norm if norm > 0 else None
+        res["rel_l2_fp32_vs_fp64_at_peak_norm"] = at_peak
+        res["final_error_over_peak_norm"] = diff / peak if peak > 0 else None
+        res["final_norm_over_peak_norm"] = norm / peak if peak > 0 else None
+        out[name] = res
+    return out
 
 
 def run_adjoint(local_rank: int) -> dict:

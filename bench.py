@@ -164,6 +164,23 @@ def time_steps(sim, torch, steps: int, stream) -> tuple[float, int]:
     return start.elapsed_time(stop) / 1e3, sim.launches - L0
 
 
+def max_over_ranks(t: float, dist, device: str) -> float:
+    """The largest of the ranks' device times (the job's time); `dist` is
+    torch.distributed or None for one process."""
+    if dist is None:
+        return t
+    import torch
+    x = torch.tensor([t], device=device, dtype=torch.float64)
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def replica_value(cells: int, steps: int, t_max: float, world: int) -> float:
+    """Whole-job Gcell-updates/s: every rank runs its own replica of the
+    workload (weak scaling), timed by the slowest rank."""
+    return world * cells * steps / t_max / 1e9
+
+
 def run_ours(args) -> dict:
     import torch
     from mpulse_b200 import runtime
@@ -200,13 +217,9 @@ def run_ours(args) -> dict:
         dt_dev, launches = time_steps(sim, torch, args.steps, stream)
     clocks = clk.summary()
     barrier()
-    t_max = dt_dev
-    if dist is not None:
-        t = torch.tensor([dt_dev], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(dt_dev, dist, "cuda")
     cells = cfg.nx * cfg.ny * cfg.nz
-    value = world * cells * args.steps / t_max / 1e9
+    value = replica_value(cells, args.steps, t_max, world)
     # FP32 state after warmup + steps, compared below with the FP64 form
     fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
     # FollowMax of Ex along z through the beam axis, over the next steps

@@ -305,22 +305,27 @@ int mp_field_energy(mp_ctx *ctx, double *energy);
  *
  * What it does: the same two kernels as mp_field_energy on caller-owned
  * device arrays.  fields[0..5] are Ex Ey Ez Bx By Bz in the plane layout
- * above ((nz+2) * ny * nx elements each, elem_bytes 4 for FP32 or 8 for FP64);
- * the interior planes 1..nz are summed, times dx dy dz, in FP64.  Work goes to
- * cuda_stream (NULL: the legacy default stream); the call waits for it and
- * writes the result to the host double *energy.
+ * above ((nz+2) * ny * nx elements each, elem_bytes 4 for FP32 or 8 for FP64),
+ * on the current device or one it can read as a peer; a pointer that is not
+ * device or managed memory is rejected with MP_ERR_INVALID before anything
+ * is launched.  The interior planes 1..nz are summed, times dx dy dz, in FP64.
+ * Work goes to cuda_stream and the call blocks until that stream has drained
+ * (cudaStreamSynchronize), then writes the result to the host double *energy.
+ * A NULL cuda_stream is the legacy default stream, which also waits for and
+ * holds up the other blocking streams of the device.  Because it blocks, it
+ * cannot be used while cuda_stream is being captured into a CUDA graph.
  *
  * Limit: the scratch is a fixed array compiled into the library
  * (MP_NOALLOC_MAX_PLANES + 32 doubles, about 130 KB, held by every GPU that
  * loads the library until the process exits), one partial sum per z-plane, so
  * nz above MP_NOALLOC_MAX_PLANES is rejected with MP_ERR_INVALID and a message
  * from mp_last_error(NULL, ..).  It allocates nothing: no cudaMalloc, no
- * cudaFree, no allocating library call.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) once for that device;
- * make that first call before any stream capture.  All calls share the array
- * and it keeps the last call's contents (nothing in it needs to start at
- * zero); calls whose work overlaps on the GPU race on it and must be
- * serialised by the caller. */
+ * cudaFree, no allocating library call.  Every call looks up the array's
+ * device address on the current device (cudaGetSymbolAddress, which neither
+ * allocates nor synchronises), so it stays valid across cudaDeviceReset.
+ * All calls share the array and it keeps the last call's contents (nothing in
+ * it needs to start at zero); calls whose work overlaps on the GPU race on it
+ * and must be serialised by the caller. */
 int mp_field_energy_noalloc(const void *const fields[6], int elem_bytes, int nx, int ny, int nz,
                             double dx, double dy, double dz, void *cuda_stream, double *energy);
 

@@ -11,6 +11,7 @@ import math
 MP_ABI_VERSION = 1
 MP_MAX_POLES = 3
 MP_MAX_SOURCES = 4
+MP_NOALLOC_MAX_PLANES = 16384
 
 # mp_status
 MP_OK = 0

@@ -15,7 +15,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 namespace mpb {
 
@@ -104,26 +103,32 @@ static __device__ __align__(256) double g_energy_scratch[MP_NOALLOC_MAX_PLANES +
 
 namespace {
 
-const int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-double *g_scratch_addr[kMaxDevices];  // device address of g_energy_scratch, per device
-
 // The host-side name g_energy_scratch is a stand-in, not a device address;
-// the address comes from cudaGetSymbolAddress with the device current.
+// the address comes from cudaGetSymbolAddress with the device current.  It is
+// looked up on every call (no allocation, no device synchronisation), so a
+// call after cudaDeviceReset, which reloads the module, gets the new address.
 cudaError_t scratch_for_current_device(double **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_energy_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_energy_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = static_cast<double *>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<double *>(p);
   return cudaSuccess;
+}
+
+// True when ptr is device (or managed) memory that the current device can
+// read: a host pointer handed to the kernel would fault the GPU, so it is
+// turned into MP_ERR_INVALID here, before any launch.
+bool device_readable(const void *ptr, int dev) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();  // the failed query leaves a (non-sticky) error behind: clear it
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  if (a.type != cudaMemoryTypeDevice) return false;
+  if (a.device == dev) return true;
+  int peer = 0;
+  return cudaDeviceCanAccessPeer(&peer, dev, a.device) == cudaSuccess && peer;
 }
 
 }  // namespace
@@ -155,8 +160,19 @@ extern "C" int mp_field_energy_noalloc(const void *const fields[6], int elem_byt
     mpb::set_global_error(msg);
     return MP_ERR_INVALID;
   }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) {
+    for (int c = 0; c < 6; ++c)
+      if (!device_readable(fields[c], dev)) {
+        snprintf(msg, sizeof msg,
+                 "mp_field_energy_noalloc: fields[%d] is not device memory readable by device %d", c, dev);
+        mpb::set_global_error(msg);
+        return MP_ERR_INVALID;
+      }
+  }
   double *scratch = nullptr;
-  cudaError_t e = scratch_for_current_device(&scratch);
+  if (e == cudaSuccess) e = scratch_for_current_device(&scratch);
   if (e == cudaSuccess) {
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     double *result = scratch + MP_NOALLOC_MAX_PLANES;

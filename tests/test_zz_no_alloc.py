@@ -63,7 +63,7 @@ def test_noalloc_rejects_too_many_planes():
         for q, n in enumerate(abi.FIELD_NAMES):
             ptrs[q] = g.device_field(n)[0]
         out = C.c_double()
-        rc = runtime.lib().mp_field_energy_noalloc(ptrs, 8, cfg.nx, cfg.ny, abi_max_planes() + 1, 1.0, 1.0, 1.0,
+        rc = runtime.lib().mp_field_energy_noalloc(ptrs, 8, cfg.nx, cfg.ny, abi.MP_NOALLOC_MAX_PLANES + 1, 1.0, 1.0, 1.0,
                                                    None, C.byref(out))
         assert rc == abi.MP_ERR_INVALID
         buf = C.create_string_buffer(256)
@@ -71,5 +71,24 @@ def test_noalloc_rejects_too_many_planes():
         assert b"exceeds" in buf.value
 
 
-def abi_max_planes() -> int:
-    return 16384  # MP_NOALLOC_MAX_PLANES in include/mpulse_b200.h
+def test_noalloc_rejects_host_pointers():
+    """A host buffer in fields[] is turned into MP_ERR_INVALID on the host,
+    before any kernel is launched (nothing reaches the GPU)."""
+    import numpy as np
+    cfg = make_case("plain_periodic", abi.MP_FP64)
+    host = np.zeros(cfg.field_count())
+    with runtime.Simulation(cfg) as g:
+        ptrs = (C.c_void_p * 6)()
+        for q, n in enumerate(abi.FIELD_NAMES):
+            ptrs[q] = g.device_field(n)[0]
+        ptrs[4] = host.ctypes.data
+        out = C.c_double()
+        rc = runtime.lib().mp_field_energy_noalloc(ptrs, 8, cfg.nx, cfg.ny, cfg.nz, 1.0, 1.0, 1.0, None,
+                                                   C.byref(out))
+        assert rc == abi.MP_ERR_INVALID
+        buf = C.create_string_buffer(256)
+        runtime.lib().mp_last_error(None, buf, 256)
+        assert b"fields[4]" in buf.value
+        # the library stays usable: a valid call right after it succeeds
+        ptrs[4] = g.device_field("By")[0]
+        assert _noalloc_energy(g) == pytest.approx(g.field_energy(), rel=1e-13, abs=0.0)

@@ -4,18 +4,27 @@
 Workload: PLRC + Kerr + CPML at 256 x 256 x 512 cells (two-pole Lorentz medium
 with chi3 E0^2 = 0.01 for z >= 64, 12-cell CPML on all six faces, focused
 Gaussian pulse injected by the paraxial short-pulse closed form), FP32 device
-state.  One "step" is one MPulse time step (E half + B half) over the whole
-grid.  The metric is Gcell-updates/s = nx ny nz x steps / time.
+state, dt = 0.45 dx / c.  One "step" is one MPulse time step (E half + B half)
+over the whole grid.  The metric is Gcell-updates/s = nx ny nz x steps / time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-`value` is timed with CUDA events on the simulation's stream, state resident in
-HBM (4.7 GB, larger than the 126 MB L2, so no L2 flush is needed).  `e2e` is the
-same metric through the C ABI with host buffers: upload of the six fields from
-pinned host memory, K steps, download of E, all inside the timed region.
-The FP64 form runs the same steps beside it, and the relative L2 error of the
-FP32 fields against it is reported.  With N > 1 every rank runs its own
-independent simulation (replicas only: the path is not sharded).
+The FP32 and FP64 forms run side by side from time 0 (both contexts live at
+once).  An untimed pre-roll of PREROLL_STEPS steps brings the pulse into the
+Kerr medium; after W warm-up steps, `value` times K steps of the FP32 form with
+CUDA events on the simulation's stream (state 4.7 GB, larger than the 126 MB
+L2, so no L2 flush is needed), plus the device time of the injection planes of
+those K steps, measured on their own and added pro rata (the planes are
+computed ahead in batches on a second stream and overlap the step kernels;
+the addition gives no credit for that overlap).  The E half-step kernel counts
+its Kerr solves and Newton iterations on the device during the timed steps.
+`e2e` is the same metric through the C ABI with host buffers: upload of the
+six fields from pinned host memory, K steps, download of E, all inside the
+timed region.  Both forms then continue to step 4000 (the workload's run
+length), with FollowMax (followmax.cpp:73-113) of Ex along the beam axis after
+every step and the relative L2 error of E (FP32 against FP64) and the peak
+|E|^2 every 50 steps.  With N > 1 every rank runs its own independent
+simulation (replicas only: the path is not sharded).
 """
 from __future__ import annotations
 
@@ -27,7 +36,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -41,8 +49,26 @@ WORKLOAD = dict(nx=256, ny=256, nz=512)
 WORKLOAD_NAME = "plrc_kerr_cpml_focused_256x256x512"
 METRIC = "Gcell-updates/s FP32 vs FP64 at rel-L2<=1e-5; adjoint/forward time ratio"
 UNIT = "Gcell-updates/s"
-# Process::time at which the timed steps start: the pulse is being injected then.
-START_TIME = 700
+# Untimed steps from time 0 before the warm-up.  The pulse (20 fs FWHM, field
+# 1/e half-width T = 5.09 um / c) peaks on the injection plane z = 20 at
+# t = 3 T (848 steps of dt = 0.018 um / c), reaches the medium at z = 64 about
+# 98 steps later and then moves about one cell per 3.3 steps (group index about
+# 1.47): at step 1100 its peak is some 47 cells into the Kerr medium, and the
+# field is non-zero in every medium cell.
+PREROLL_STEPS = 1100
+ACCURACY_STEPS = 4000     # run length of the workload
+RECORD_EVERY = 50         # FP32-vs-FP64 error and peak |E|^2 sampled this often
+
+
+def workload_config_keys(cfg: abi.Config) -> dict:
+    """The `config` object of both arms' lines: the workload itself."""
+    return {"workload": WORKLOAD_NAME, "grid": [cfg.nx, cfg.ny, cfg.nz], "solver": "fdtd-plrc-nonlin",
+            "poles": 2, "chi3_E0^2": cfg.chi, "cpml": f"all faces, d={cfg.cpml_d}",
+            "source": "short_pulse_inject (focused, waist 2 um at z=200, 20 fs, injected at z=20)",
+            "dx_um": cfg.dx,
+            "dt": f"{configs.MEDIUM_COURANT} dx/c = {cfg.dt:g} um/c (0.5 dx/c amplifies grid noise with this "
+                  f"medium in the reference scheme as well; pinned by tests/test_stability.py)",
+            "l2": "state 4.7 GB (FP32) > 126 MB L2, no flush needed"}
 
 
 def bench_config(precision: int) -> abi.Config:
@@ -139,15 +165,87 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def follow_trace(sim, axis, z_start: int, steps: int = 16) -> list:
-    """FollowMax::calculate (followmax.cpp:73-113) of Ex along z through the
-    column `axis`, after each of `steps` steps (mp_follow_max)."""
-    ip, out = z_start, []
-    for _ in range(steps):
-        sim.step(1)
-        ip, x = sim.follow_max("Ex", 2, (axis[0], axis[1], ip), ip)
-        out.append(x)
-    return out
+def device_array(sim, name: str, torch):
+    """A torch view (no copy) of one field's device array, for the FP32-vs-FP64
+    comparisons of the measurement (mp_device_field)."""
+    ptr, count, elem = sim.device_field(name)
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (count,), "typestr": "<f4" if elem == 4 else "<f8",
+                                    "data": (ptr, False), "strides": None, "version": 2}
+
+    return torch.as_tensor(_View(), device="cuda")
+
+
+class PairRun:
+    """The FP32 and FP64 forms of the workload stepped in lockstep.  After every
+    step of advance() it runs FollowMax (mp_follow_max, followmax.cpp:73-113)
+    of Ex along z through the beam axis on both, from the injection plane on;
+    every RECORD_EVERY steps it records the relative L2 error of E (FP32
+    against FP64, over all stored cells), the FP64 field norm and the peak
+    |E|^2 of both forms (device reductions in FP64)."""
+
+    def __init__(self, sim32, sim64, cfg, torch):
+        self.s32, self.s64, self.torch = sim32, sim64, torch
+        self.axis = (cfg.nx // 2, cfg.ny // 2)
+        self.start = cfg.sources[0].distance
+        self.ip = {32: self.start, 64: self.start}
+        self.pos = {32: float(self.ip[32]), 64: float(self.ip[64])}
+        self.records = []
+
+    def follow(self):
+        for tag, sim in ((32, self.s32), (64, self.s64)):
+            self.ip[tag], self.pos[tag] = sim.follow_max("Ex", 2, (self.axis[0], self.axis[1], self.ip[tag]),
+                                                         self.ip[tag])
+
+    def compare(self) -> dict:
+        torch = self.torch
+        torch.cuda.synchronize()
+        e32 = [device_array(self.s32, n, torch) for n in ("Ex", "Ey", "Ez")]
+        e64 = [device_array(self.s64, n, torch) for n in ("Ex", "Ey", "Ez")]
+        diff = sum(float(torch.sum((a.double() - b) ** 2)) for a, b in zip(e32, e64))
+        norm = sum(float(torch.sum(b * b)) for b in e64)
+        i32 = float(torch.max(sum(a.double() ** 2 for a in e32)))
+        i64 = float(torch.max(sum(b * b for b in e64)))
+        return {"diff": math.sqrt(diff), "norm": math.sqrt(norm), "peak_I32": i32, "peak_I64": i64}
+
+    def record(self):
+        c = self.compare()
+        self.records.append({"step": self.s32.time, "rel_l2": c["diff"] / c["norm"] if c["norm"] > 0 else None,
+                             "norm": c["norm"], "err": c["diff"], "peak_I32": c["peak_I32"], "peak_I64": c["peak_I64"],
+                             "follow32": self.pos[32], "follow64": self.pos[64]})
+
+    def advance(self, steps: int):
+        for _ in range(steps):
+            self.s32.step_async(1)
+            self.s64.step_async(1)
+            self.follow()
+            if self.s32.time % RECORD_EVERY == 0:
+                self.s32.check_status()
+                self.s64.check_status()
+                self.record()
+
+    def summary(self) -> dict:
+        recs = [r for r in self.records if r["norm"] > 0]
+        peak = max(recs, key=lambda r: r["norm"])
+        last = self.records[-1]
+        return {
+            "steps": last["step"], "record_every": RECORD_EVERY,
+            "rel_l2_fp32_vs_fp64_final": last["rel_l2"],
+            "rel_l2_fp32_vs_fp64_max": max(r["rel_l2"] for r in recs),
+            "rel_l2_fp32_vs_fp64_at_peak_norm": peak["rel_l2"], "peak_norm_step": peak["step"],
+            "final_error_over_peak_norm": last["err"] / peak["norm"],
+            "final_norm_over_peak_norm": last["norm"] / peak["norm"],
+            "followmax": {"field": "Ex", "dim": "z", "line_xy": list(self.axis), "every_step": True,
+                          "start_z": self.start,
+                          "max_abs_diff_cells": max(abs(r["follow32"] - r["follow64"]) for r in self.records),
+                          "trace": [[r["step"], round(r["follow32"], 4), round(r["follow64"], 4)]
+                                    for r in self.records]},
+            "peak_intensity": {"what": "max over the grid of Ex^2 + Ey^2 + Ez^2",
+                               "max_rel_diff": max(abs(r["peak_I32"] - r["peak_I64"]) / r["peak_I64"]
+                                                   for r in recs if r["peak_I64"] > 0),
+                               "trace": [[r["step"], r["peak_I32"], r["peak_I64"]] for r in self.records]},
+        }
 
 
 def time_steps(sim, torch, steps: int, stream) -> tuple[float, int]:
@@ -200,35 +298,51 @@ def run_ours(args) -> dict:
 
     cfg = bench_config(abi.MP_FP32)
     cfg.device = local_rank
+    cfg64 = bench_config(abi.MP_FP64)
+    cfg64.device = local_rank
     stream = torch.cuda.Stream()
     sim = runtime.Simulation(cfg)
-    sim.set_stream(stream.cuda_stream)
-    sim.time = START_TIME
-    # warm-up
-    sim.step(args.warmup)
+    sim64 = runtime.Simulation(cfg64)
+    for g in (sim, sim64):
+        g.set_stream(stream.cuda_stream)
+    pair = PairRun(sim, sim64, cfg, torch)
+    # untimed pre-roll from time 0, then the warm-up
+    pair.advance(args.preroll)
+    pair.advance(args.warmup)
 
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
 
+    cells = cfg.nx * cfg.ny * cfg.nz
+    sim.kerr_counts()  # reset the device counters
     barrier()
     with ClockSampler(local_rank) as clk:
         dt_dev, launches = time_steps(sim, torch, args.steps, stream)
     clocks = clk.summary()
+    kerr_solves, kerr_iters = sim.kerr_counts()
     barrier()
-    t_max = max_over_ranks(dt_dev, dist, "cuda")
-    cells = cfg.nx * cfg.ny * cfg.nz
+    t0_window = sim.time - args.steps
+    sim64.kerr_counts()
+    dt64, _ = time_steps(sim64, torch, args.steps, stream)
+    kerr64 = sim64.kerr_counts()
+    pair.follow()
+    state = pair.compare()
+    # per-kernel device times (CUDA events around each launch, further steps,
+    # the same number on both forms so they stay in lockstep)
+    nkt = max(3, min(args.steps, 10))
+    kt = sim.kernel_times(nkt)
+    kt64 = sim64.kernel_times(nkt)
+    pair.follow()
+    # the injection planes of the timed steps were computed before the window:
+    # their device time, pro rata
+    src_s = args.steps * kt["sources_ms"] / 1e3
+    src64_s = args.steps * kt64["sources_ms"] / 1e3
+    t_max = max_over_ranks(dt_dev + src_s, dist, "cuda")
     value = replica_value(cells, args.steps, t_max, world)
-    # FP32 state after warmup + steps, compared below with the FP64 form
-    fp32_state = {n: sim.download(n) for n in ("Ex", "Ey", "Ez")}
-    # FollowMax of Ex along z through the beam axis, over the next steps
-    axis = (cfg.nx // 2, cfg.ny // 2)
-    z_start = int(np.argmax(np.abs(fp32_state["Ex"][1:-1, axis[1] - 1, axis[0] - 1]))) + 1
-    trace32 = follow_trace(sim, axis, z_start)
+    value64 = world * cells * args.steps / (dt64 + src64_s) / 1e9
 
-    # per-kernel device times (CUDA events around each launch, further steps)
-    kt = sim.kernel_times(max(3, min(args.steps, 10)))
     alg = algorithmic_bytes(cfg, 4)
     peaks = measured_peaks()
     e_ms = kt["e_half_ms"]
@@ -244,45 +358,46 @@ def run_ours(args) -> dict:
                 "algorithmic_bytes_per_launch": alg["e_half"], "launch_ms": round(e_ms, 4)}
     step_achieved = alg["step"] / (t_max / args.steps) / 1e9
     step_roofline = {"achieved": round(step_achieved, 1), "frac": round(step_achieved / peaks["hbm_gbs"], 4),
-                     "algorithmic_bytes_per_step": alg["step"], "unit": "GB/s"}
+                     "algorithmic_bytes_per_step": alg["step"], "unit": "GB/s",
+                     "what": "step bytes / (window + sources pro rata) per step"}
 
-    # FP64 form on the same steps, and the FP32 error against it
+    # end to end through the C ABI with host buffers (FP32 form), then the same
+    # steps on the FP64 form to keep the pair in lockstep
+    e2e = run_e2e(args, torch, sim, cfg)
+    sim64.step(args.steps)
+    pair.follow()
+    # both forms on to the end of the workload's run
+    pair.advance(max(0, ACCURACY_STEPS - sim.time))
+    accuracy = pair.summary()
     sim.close()
-    torch.cuda.empty_cache()
-    cfg64 = bench_config(abi.MP_FP64)
-    cfg64.device = local_rank
-    sim64 = runtime.Simulation(cfg64)
-    sim64.set_stream(stream.cuda_stream)
-    sim64.time = START_TIME
-    sim64.step(args.warmup)
-    dt64, _ = time_steps(sim64, torch, args.steps, stream)
-    fp64_state = {n: sim64.download(n) for n in ("Ex", "Ey", "Ez")}
-    trace64 = follow_trace(sim64, axis, z_start)
     sim64.close()
-    num = sum(float(np.sum((fp32_state[n] - fp64_state[n]) ** 2)) for n in fp32_state)
-    den = sum(float(np.sum(fp64_state[n] ** 2)) for n in fp64_state)
-    rel = math.sqrt(num / den) if den > 0 else None
-    value64 = world * cells * args.steps / dt64 / 1e9
+    torch.cuda.empty_cache()
 
-    # end to end through the C ABI with host buffers
-    e2e = run_e2e(args, torch, stream, local_rank)
     adjoint = run_adjoint(local_rank) if rank == 0 else None
     others = run_other_configs(local_rank, torch, stream) if rank == 0 else None
 
+    n_med = alg["N_med"]
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "grid": [cfg.nx, cfg.ny, cfg.nz], "solver": "fdtd-plrc-nonlin",
-                   "poles": 2, "cpml": "all faces, d=12", "source": "short_pulse_inject (focused, waist 2 um)",
-                   "start_time": START_TIME, "parallelism": f"replicas{world}",
-                   "l2": "state 4.7 GB > 126 MB L2, no flush needed"},
-        "fp64": {"value": round(value64, 4), "unit": UNIT, "ms_per_step": round(dt64 / args.steps * 1e3, 4)},
+        "config": workload_config_keys(cfg),
+        "parallelism": f"replicas{world}",
+        "state": {"what": f"untimed pre-roll of {args.preroll} steps from time 0 and {args.warmup} warm-up steps "
+                          f"(FP32 and FP64 side by side): the pulse is in the Kerr medium",
+                  "first_timed_step": t0_window,
+                  "kerr_solves_per_step": kerr_solves / args.steps,
+                  "newton_iterations_per_solve": kerr_iters / kerr_solves if kerr_solves else None,
+                  "medium_cells": n_med, "kerr_solves_over_medium_cells": kerr_solves / args.steps / n_med,
+                  "fp64_kerr_solves_per_step": kerr64[0] / args.steps},
+        "window": {"device_s": round(dt_dev, 6), "sources_pro_rata_s": round(src_s, 6),
+                   "what": "value = cells x steps / (window device time + sources_ms x steps)"},
+        "fp64": {"value": round(value64, 4), "unit": UNIT, "ms_per_step": round((dt64 + src64_s) / args.steps * 1e3, 4),
+                 "kernel_ms": kt64},
         "fp32_over_fp64": round(value / value64, 3) if value64 > 0 else None,
-        "rel_l2_fp32_vs_fp64": rel,
-        "followmax": {"field": "Ex", "dim": "z", "line_xy": list(axis), "steps": len(trace32),
-                      "fp32": [round(x, 4) for x in trace32], "fp64": [round(x, 4) for x in trace64],
-                      "max_abs_diff": float(np.max(np.abs(np.array(trace32) - np.array(trace64))))},
+        "rel_l2_fp32_vs_fp64": state["diff"] / state["norm"] if state["norm"] > 0 else None,
+        "rel_l2_at_step": sim_time_after(t0_window, args),
+        "accuracy_4000_steps": accuracy,
         "adjoint_forward_ratio": adjoint["fp32"]["ratio"] if adjoint else None,
         "adjoint": adjoint,
         "other_workloads": others,
@@ -298,6 +413,12 @@ def run_ours(args) -> dict:
         dist.barrier()
         dist.destroy_process_group()
     return out if rank == 0 else None
+
+
+def sim_time_after(t0_window: int, args) -> int:
+    """The time both forms reach after the two timed windows (where
+    rel_l2_fp32_vs_fp64 is taken)."""
+    return t0_window + args.steps
 
 
 def run_other_configs(local_rank: int, torch, stream) -> dict:
@@ -466,7 +587,10 @@ def run_adjoint_large(args) -> dict:
 
 
 def run_profile(args) -> dict:
-    """FP32 workload only: warm-up, then the timed steps; no other kernels."""
+    """FP32 workload only: pre-roll, warm-up, then the timed steps; no other
+    kernels (for ncu captures: the E half's launches are the odd ones from
+    launch 2 (args.preroll + args.warmup) on, counting one source batch per 64
+    steps)."""
     import torch
     from mpulse_b200 import runtime
     torch.cuda.set_device(0)
@@ -474,27 +598,30 @@ def run_profile(args) -> dict:
     stream = torch.cuda.Stream()
     sim = runtime.Simulation(cfg)
     sim.set_stream(stream.cuda_stream)
-    sim.time = START_TIME
-    sim.step(args.warmup)
+    sim.step(args.preroll + args.warmup)
+    L0 = sim.launches
+    sim.kerr_counts()
     dt, launches = time_steps(sim, torch, args.steps, stream)
+    solves, iters = sim.kerr_counts()
     cells = cfg.nx * cfg.ny * cfg.nz
     kt = sim.kernel_times(5)
     sim.close()
-    return {"profile_run": True, "grid": [cfg.nx, cfg.ny, cfg.nz], "steps": args.steps,
-            "value": cells * args.steps / dt / 1e9, "unit": UNIT, "gpu_launches": launches, "kernel_ms": kt}
+    return {"profile_run": True, "grid": [cfg.nx, cfg.ny, cfg.nz], "steps": args.steps, "preroll": args.preroll,
+            "launches_before_window": L0, "value": cells * args.steps / dt / 1e9, "unit": UNIT,
+            "gpu_launches": launches, "kerr_solves_per_step": solves / args.steps,
+            "newton_iterations_per_solve": iters / solves if solves else None, "kernel_ms": kt}
 
 
-def run_e2e(args, torch, stream, local_rank) -> dict:
-    from mpulse_b200 import runtime
-    cfg = bench_config(abi.MP_FP32)
-    cfg.device = local_rank
+def run_e2e(args, torch, sim, cfg) -> dict:
+    """The metric through the C ABI with host buffers, on the simulation's
+    current state: mp_upload of the six fields from pinned host memory (the
+    state itself, downloaded before the timed region), mp_step(K), mp_download
+    of Ex, Ey, Ez, timed by the wall clock."""
     count = cfg.field_count()
     host_in = {n: torch.zeros(count, dtype=torch.float64, pin_memory=True).numpy() for n in abi.FIELD_NAMES}
     host_out = {n: torch.zeros(count, dtype=torch.float64, pin_memory=True).numpy() for n in ("Ex", "Ey", "Ez")}
-    sim = runtime.Simulation(cfg)
-    sim.set_stream(stream.cuda_stream)
-    sim.time = START_TIME
-    sim.step(1)  # first launch out of the timed region
+    for n in abi.FIELD_NAMES:
+        sim.download(n, host_in[n])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for n in abi.FIELD_NAMES:
@@ -503,11 +630,10 @@ def run_e2e(args, torch, stream, local_rank) -> dict:
     for n in ("Ex", "Ey", "Ez"):
         sim.download(n, host_out[n])
     t1 = time.perf_counter()
-    sim.close()
     cells = cfg.nx * cfg.ny * cfg.nz
     return {"value": round(cells * args.steps / (t1 - t0) / 1e9, 4), "unit": UNIT,
             "h2d_bytes_per_step": int(6 * count * 8 / args.steps), "d2h_bytes_per_step": int(3 * count * 8 / args.steps),
-            "what": "mp_upload x6 (pinned double) + mp_step(K) + mp_download x3, wall clock"}
+            "what": "mp_upload x6 (pinned double) + mp_step(K) + mp_download x3 on the pre-rolled state, wall clock"}
 
 
 # ---------------------------------------------------------------------------
@@ -521,32 +647,47 @@ def _ref_binary():
     return None
 
 
+def reference_state_init(cfg: abi.Config) -> str:
+    """pulse_init block (GaussPulseInit, pulseinit.cpp:7-74) of the state the
+    reference is timed on: a By/Ex Gaussian pulse with the workload's carrier
+    (800 nm), waist (2 um) and length (20 fs FWHM) centred at z = 111, where
+    the pre-rolled state of the GPU arm has its peak; as there, the field is
+    non-zero in every medium cell, so every cell takes the Kerr solve."""
+    k0 = 2 * math.pi / 0.8
+    z0 = configs.field_fwhm_to_t0(20.0)  # spatial 1/e half-width c T
+    return (f"pulse_init {{ k {k0!r} r0 2.0 z0 {z0!r} zc {111 * cfg.dz!r} C 0 Bx 0 By 1 bound 0 }}")
+
+
 def reference_slabs(steps: int, warmup: int, procs: int) -> dict:
-    """Runs the reference build on the bench workload split into `procs`
-    independent z-slabs (MPulse's own slab decomposition without the halo
-    exchange, one process per core, as its MPI build would run them) for
-    warmup + steps steps, and returns the aggregate rate of the timed steps."""
+    """Runs the reference build on the bench workload as `procs` z-slab
+    processes, MPulse's own slab decomposition of its MPI build
+    (mpi_bound.cpp:66-109) without the halo exchange: each process holds the
+    planes of its slab of the one 256 x 256 x 512 grid (the harness's
+    slab_xy_periodic boundary), so the CPML z faces, the injection plane and
+    the vacuum / medium split sit only in the slabs that contain them and the
+    processes together do the whole grid's per-cell work.  Every slab starts
+    from reference_state_init, runs warmup + steps steps, and times the last
+    `steps`; returns the aggregate rate (all cells over the slowest process's
+    time) and the median per-process rate."""
     from oracle import pyoracle
     binary = _ref_binary()
     cfg = bench_config(abi.MP_FP64)
-    nz_slab = max(2 * cfg.cpml_d, cfg.nz // procs)
-    procs = max(1, cfg.nz // nz_slab)
+    nz_slab = max(-(-cfg.nz // procs), cfg.cpml_d + 1)  # a slab holds at most one z face
+    slabs = [(z, min(z + nz_slab - 1, cfg.nz)) for z in range(1, cfg.nz + 1, nz_slab)]
     tmp = tempfile.mkdtemp(prefix="mpref_bench_")
+    init = reference_state_init(cfg)
     runs = []
-    for p in range(procs):
-        c = bench_config(abi.MP_FP64)
-        c.nz = nz_slab
-        c.medium_z0 = 0 if p > 0 else cfg.medium_z0
-        c.medium_z1 = nz_slab + 1
+    for p, (z0, z1) in enumerate(slabs):
         d = os.path.join(tmp, f"r{p}")
         os.makedirs(d)
         with open(os.path.join(d, "setup.dat"), "w") as f:
-            f.write(pyoracle.setup_text(c, warmup + steps))
+            f.write(pyoracle.setup_text(cfg, warmup + steps, inits=init,
+                                        boundary=f"slab_xy_periodic {{ z0 {z0} z1 {z1} }}"))
         env = dict(os.environ, MPULSE_REF_WARMUP=str(warmup))
-        runs.append((subprocess.Popen([binary, os.path.join(d, "setup.dat"), d], stdout=subprocess.PIPE,
-                                      stderr=subprocess.DEVNULL, env=env, text=True), c))
+        runs.append(subprocess.Popen([binary, os.path.join(d, "setup.dat"), d], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, env=env, text=True))
     secs, cells, rates = [], 0, []
-    for pr, c in runs:
+    for pr in runs:
         outp, _ = pr.communicate()
         if pr.returncode != 0:
             raise RuntimeError("reference run failed")
@@ -555,20 +696,26 @@ def reference_slabs(steps: int, warmup: int, procs: int) -> dict:
         cells += r["cells"]
         rates.append(r["cells"] * steps / r["seconds"] / 1e9)
     t = max(secs)
-    return {"value": cells * steps / t / 1e9, "procs": procs, "cells": cells, "seconds": t, "nz_slab": nz_slab,
-            "per_core": float(np.median(rates))}
+    return {"value": cells * steps / t / 1e9, "procs": len(slabs), "cells": cells, "seconds": t,
+            "nz_slab": nz_slab, "per_core": float(np.median(rates))}
+
+
+def _reference_sample_text(r: dict, warmup: int, steps: int) -> str:
+    return (f"MPulse reference build (-O3), the one 256x256x512 grid of the workload as {r['procs']} z-slab processes "
+            f"of {r['nz_slab']} planes (MPulse's MPI slab split without the halo exchange; CPML faces and "
+            f"injection plane only where the grid has them), from a pulse_init state in the Kerr medium, "
+            f"{warmup} warm-up + {steps} timed steps")
 
 
 def cpu_baseline_sample(args) -> dict:
     """Bounded CPU baseline for the headline line: the reference build on the
-    host cores for 2 timed steps of the full workload, split into z-slabs."""
+    host cores for 2 timed steps of the full workload, as z-slabs."""
     if _ref_binary() is None:
         return cpu_baseline_port()
     procs = max(1, min(os.cpu_count() or 1, 64))
     r = reference_slabs(steps=2, warmup=1, procs=procs)
     return {"value": round(r["value"], 6), "unit": UNIT, "cores": r["procs"], "kind": "reference",
-            "sample": f"MPulse reference build (-O3), full 256x256x512 workload as {r['procs']} independent "
-                      f"z-slabs of {r['nz_slab']} planes, 1 warm-up + 2 timed steps",
+            "sample": _reference_sample_text(r, 1, 2), "same_config": True,
             "per_core_value": round(r["per_core"], 6),
             "per_core": "median rate of one slab process (the reference is single-threaded), measured while all ran"}
 
@@ -579,7 +726,6 @@ def cpu_baseline_port() -> dict:
     c.nz = 32
     c.medium_z0 = 0
     o = pyoracle.OracleSim(c)
-    o.time = START_TIME
     t0 = time.perf_counter()
     o.step(2)
     t = time.perf_counter() - t0
@@ -598,14 +744,16 @@ def run_reference_arm(args) -> dict | None:
     r = reference_slabs(steps=args.steps, warmup=args.warmup, procs=procs)
     wall = time.perf_counter() - t0
     v = round(r["value"], 6)
-    sample = (f"MPulse reference build (-O3), the {WORKLOAD_NAME} workload as {r['procs']} independent z-slab "
-              f"processes of {r['nz_slab']} planes, {args.warmup} warm-up + {args.steps} timed steps")
+    cfg = bench_config(abi.MP_FP64)
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(r["seconds"] / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "grid": [256, 256, 512], "parallelism": f"{r['procs']} processes"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["procs"], "kind": "reference", "sample": sample},
+        "config": workload_config_keys(cfg),
+        "parallelism": f"{r['procs']} processes",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["procs"], "kind": "reference",
+                         "sample": _reference_sample_text(r, args.warmup, args.steps), "same_config": True,
+                         "per_core_value": round(r["per_core"], 6)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 2),
     }
@@ -616,6 +764,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--preroll", type=int, default=PREROLL_STEPS,
+                    help="untimed steps from time 0 before the warm-up (pulse into the Kerr medium)")
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--profile-only", action="store_true",

@@ -340,6 +340,16 @@ long long mp_launch_count(mp_ctx *ctx);
 int mp_kernel_times(mp_ctx *ctx, int n_steps, double *e_half_ms, double *b_half_ms,
                     double *sources_ms);
 
+/* The Kerr solves of the E half-steps run since the previous call (or since
+ * mp_create), read from counters the E-half kernel keeps on the device: the
+ * cell updates in which the Newton solve for |E| ran (FDTD_PLRCNonlinCore::
+ * plrcStepD, src/fdtd_plrc.cpp:406-419, skips it where c = 0; the solve of
+ * FDTD_Nonlinear::stepD, src/fdtd_nl.cpp:86-92, is skipped here where D = 0)
+ * and the Newton iterations they took, summed.  Resets both counters; synchronises the context's stream.
+ * Zero for the linear solvers.  No counterpart in MPulse (a diagnostic that
+ * shows how much of a run's work was the nonlinear solve). */
+int mp_kerr_counts(mp_ctx *ctx, long long *solves, long long *iterations);
+
 /* Field initialisers (FieldSimulation's "pulse_init", "gauss_init",
  * "wave_init", src/fieldsim.cpp:157-168), evaluated on the device in FP64
  * over the stored cells: the interior x / y columns of every z plane.  MPulse

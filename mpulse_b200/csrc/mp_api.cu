@@ -118,6 +118,8 @@ struct mp_ctx {
   double *d_wcoef = nullptr;
   int *d_status = nullptr;
   int *h_status = nullptr;
+  unsigned long long *d_kerr = nullptr;  // Kerr solves and Newton iterations since the last mp_kerr_counts
+  unsigned long long *h_kerr = nullptr;
   double *staging = nullptr;
   double *d_diag = nullptr;   // diagnostics scratch: per-plane partials, then the result
   double *h_diag = nullptr;   // pinned results (two doubles)
@@ -352,6 +354,7 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
     bp.src[s].v1 = base + 3 * pl;
   }
   ep.status = c->d_status;
+  ep.kerr_count = c->d_kerr;
   bp.status = c->d_status;
   ep.n_field = bp.n_field = (long long)c->fcount;
   ep.n_psi = (long long)c->psi_cells;
@@ -699,6 +702,8 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   }
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_status), ST_COUNT * sizeof(int)), "status allocation");
   MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_status), ST_COUNT * sizeof(int)), "pinned allocation");
+  MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_kerr), 2 * sizeof(unsigned long long)), "counter allocation");
+  MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_kerr), 2 * sizeof(unsigned long long)), "pinned allocation");
   MPB_TRY(dalloc(c, reinterpret_cast<void **>(&c->d_diag), size_t(g.nz + 3) * sizeof(double)), "diagnostics allocation");
   MPB_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->h_diag), 2 * sizeof(double)), "pinned allocation");
 
@@ -1063,6 +1068,7 @@ void mp_destroy(mp_ctx *c) {
   }
   if (c->staging) cudaFree(c->staging);
   if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->h_kerr) cudaFreeHost(c->h_kerr);
   if (c->h_diag) cudaFreeHost(c->h_diag);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -1279,6 +1285,19 @@ int mp_kernel_times(mp_ctx *c, int n_steps, double *e_ms, double *b_ms, double *
   *b_ms = acc[1] / n_steps;
   *s_ms = acc[2] / n_steps;
   return mp_check_status(c);
+}
+
+int mp_kerr_counts(mp_ctx *c, long long *solves, long long *iterations) {
+  if (!c || !solves || !iterations) return MP_ERR_INVALID;
+  cudaSetDevice(c->cfg.device);
+  cudaError_t e = cudaMemcpyAsync(c->h_kerr, c->d_kerr, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_kerr, 0, 2 * sizeof(unsigned long long), c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_err(c, e, "Kerr counter read");
+  *solves = (long long)c->h_kerr[0];
+  *iterations = (long long)c->h_kerr[1];
+  return MP_OK;
 }
 
 int mp_last_error(mp_ctx *c, char *buf, size_t n) {

@@ -88,32 +88,57 @@ __device__ __forceinline__ double rcp_pos(double d) {
 }
 
 // Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
-// (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped.
+// (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped at
+// maxit iterations.  Adds the iterations it ran to *iters.
 __device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
-                                              int *status) {
+                                              int *status, unsigned *iters) {
   double Eold;
   int it = 0;
   do {
     Eold = E;
     const double E2 = E * E;
     E = (2.0 * A * E2 * E + C) * rcp_pos(3.0 * A * E2 + 1.0);
-  } while (fabs(E - Eold) > tol && ++it < maxit);
+    ++it;
+  } while (fabs(E - Eold) > tol && it < maxit);
   if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
+  *iters += unsigned(it);
   return E;
 }
 
 // FDTD_Nonlinear's Newton for eps E + chi E^3 = D (fdtd_nl.cpp:86-92).
 __device__ __forceinline__ double nl_newton(double E, double eps, double chi, double D, double tol,
-                                            int maxit, int *status) {
+                                            int maxit, int *status, unsigned *iters) {
   double Eold;
   int it = 0;
   do {
     Eold = E;
     const double E2 = E * E;
     E = (2.0 * chi * E2 * E + D) * rcp_pos(3.0 * chi * E2 + eps);
-  } while (fabs(E - Eold) > tol && ++it < maxit);
+    ++it;
+  } while (fabs(E - Eold) > tol && it < maxit);
   if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
+  *iters += unsigned(it);
   return E;
+}
+
+// Per-thread counts of the Kerr solves a thread ran ([0]: cells in which the
+// Newton solve ran, [1]: the iterations they took), added to the context's
+// counters once per warp when the thread's z-march ends.
+struct KerrCount {
+  unsigned solves = 0, iters = 0;
+};
+
+template <int MODE>
+__device__ __forceinline__ void flush_kerr_count(unsigned long long *dst, const KerrCount &kc) {
+  if (MODE != MODE_PLRC_NONLIN && MODE != MODE_NL) return;
+  const unsigned m = __activemask();
+  const unsigned a = __reduce_add_sync(m, kc.solves);
+  const unsigned b = __reduce_add_sync(m, kc.iters);
+  const int lane = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) & 31;
+  if (lane == __ffs(m) - 1 && a != 0u) {
+    atomicAdd(dst, (unsigned long long)a);
+    atomicAdd(dst + 1, (unsigned long long)b);
+  }
 }
 
 // Values one E update reads: B at the cell and its x-1, y-1, z-1 neighbours
@@ -191,7 +216,7 @@ template <typename T, int MODE, int NP, bool DESIGN = false, bool SPECIAL = true
 __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
                                        unsigned cmask, const EIn<T> &v, T ikx, T iky, T ikz,
                                        typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
-                                       T &ezn) {
+                                       T &ezn, KerrCount &kc) {
   const T dt = p.dt;
   CellCoef<T, NP> lc;
   cell_coef<T, NP, DESIGN>(p, i, j, k, med, lc);
@@ -270,7 +295,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       const double rD = rsqrt(D2);  // as in the PLRC Kerr update below
       const double D = D2 * rD;
       const double E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
-      const double E = nl_newton(E0, p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status);
+      const double E = nl_newton(E0, p.eps_d, p.chi_d, D, p.newton_tol, p.newton_max, p.status, &kc.iters);
+      ++kc.solves;
       const double sc = E * rD;
       exn = T(sc * Dx);
       eyn = T(sc * Dy);
@@ -322,7 +348,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
         const double rC = rsqrt(C2);
         const double C = C2 * rC;
         const double E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
-        const double E = kerr_newton(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status);
+        const double E = kerr_newton(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status, &kc.iters);
+        ++kc.solves;
         const double sc = E * rC;
         exn = T(sc * cx);
         eyn = T(sc * cy);

@@ -113,6 +113,7 @@ struct EParams {
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];
   int *status;
+  unsigned long long *kerr_count;  // [0] Kerr solves, [1] their Newton iterations (accumulated)
   long long n_field;      // elements of each field and history array
   long long n_psi;        // pairs of each PLRC accumulator array
 };

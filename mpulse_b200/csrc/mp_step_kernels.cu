@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
   int *const st = p.status;
   T bx_km = ldg_c(Bx, km * plane + col, nf, st);
   T by_km = ldg_c(By, km * plane + col, nf, st);
+  KerrCount kc;
 
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * plane;
@@ -141,9 +142,9 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
     }
     T exn, eyn, ezn;
     if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
-      e_cell<T, MODE, NP, DESIGN, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
+      e_cell<T, MODE, NP, DESIGN, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
     else
-      e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
+      e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
     // ---- stores
     st_c(Ex, base + col, nf, st, exn);
     st_c(Ey, base + col, nf, st, eyn);
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * 
     bx_km = v.bx;
     by_km = v.by;
   }
+  flush_kerr_count<MODE>(p.kerr_count, kc);
 }
 
 template <typename T>

@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (p.zperiodic && km == 0) km = p.nz;
   T bx_km = ld(Bx + km * plane + col);
   T by_km = ld(By + km * plane + col);
+  KerrCount kc;
 
   for (int m = 0; m < nplanes; ++m) {
     const int k = k0 + m;
@@ -265,9 +266,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     const T ikz = ld(p.ik[2] + k);
     T exn, eyn, ezn;
     if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
-      e_cell<T, MODE, NP, false, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
+      e_cell<T, MODE, NP, false, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
     else
-      e_cell<T, MODE, NP, false, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn);
+      e_cell<T, MODE, NP, false, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
     p.E[0][base + col] = exn;
     p.E[1][base + col] = eyn;
     p.E[2][base + col] = ezn;
@@ -281,6 +282,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     bx_km = v.bx;
     by_km = v.by;
   }
+  flush_kerr_count<MODE>(p.kerr_count, kc);
 }
 
 // ---- B half -----------------------------------------------------------------

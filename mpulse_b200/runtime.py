@@ -26,7 +26,7 @@ EXPORTED = (
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
     "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_state_size", "mp_save_state",
-    "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max",
+    "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max", "mp_kerr_counts",
 )
 
 _lib = None
@@ -101,6 +101,8 @@ def lib():
     L.mp_initialize.restype = C.c_int
     L.mp_follow_max.argtypes = [vp, cp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), dp]
     L.mp_follow_max.restype = C.c_int
+    L.mp_kerr_counts.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.mp_kerr_counts.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
@@ -201,6 +203,13 @@ class Simulation:
         e, b, s = C.c_double(), C.c_double(), C.c_double()
         self._check(lib().mp_kernel_times(self._h, int(n), C.byref(e), C.byref(b), C.byref(s)))
         return {"e_half_ms": e.value, "b_half_ms": b.value, "sources_ms": s.value}
+
+    def kerr_counts(self) -> tuple[int, int]:
+        """(Kerr solves, Newton iterations) of the E half-steps since the last
+        call (mp_kerr_counts); resets the device counters."""
+        a, b = C.c_longlong(), C.c_longlong()
+        self._check(lib().mp_kerr_counts(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def field_energy(self) -> float:
         """FieldEnergyDiag::calculate (fielddiag.cpp:255-286) on the device state."""

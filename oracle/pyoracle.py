@@ -223,14 +223,17 @@ def init_block(init: abi.Init) -> str:
 
 
 def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver_name: str | None = None,
-               extra: str = "", inits: str = "") -> str:
+               extra: str = "", inits: str = "", boundary: str | None = None) -> str:
     """MPulse setup file (rebuild.cpp grammar) describing `cfg`.  `solver_name`
     replaces the solver block's name (e.g. "fdtd-gpu-plrc-nonlin" for the B200
-    plug-in, which reads the same keys); `extra` is appended to its body."""
+    plug-in, which reads the same keys); `extra` is appended to its body;
+    `boundary` replaces the boundary block (e.g. the harness's
+    "slab_xy_periodic { z0 .. z1 .. }")."""
     g = (f"globals {{ grid-x {cfg.nx} grid-y {cfg.ny} grid-z {cfg.nz} "
          f"grid-dx {_fmt(cfg.dx)} grid-dy {_fmt(cfg.dy)} grid-dz {_fmt(cfg.dz)} "
          f"dt {_fmt(cfg.dt)} T-total {steps} }}\n")
-    bnd = "single_periodic { }" if cfg.boundary == abi.MP_BOUNDARY_PERIODIC else "single_xy_periodic { }"
+    bnd = boundary or ("single_periodic { }" if cfg.boundary == abi.MP_BOUNDARY_PERIODIC
+                       else "single_xy_periodic { }")
     solver = solver_name or _SOLVER_NAMES[cfg.solver]
     body = [f"eps {_fmt(cfg.eps)}"]
     if cfg.solver in (abi.MP_SOLVER_NL, abi.MP_SOLVER_PLRC_NONLIN):
@@ -302,7 +305,7 @@ def full_to_plane(cfg: abi.Config, full: np.ndarray) -> np.ndarray:
 
 def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
                   names=abi.FIELD_NAMES, binary: str = REF_BIN, workdir: str | None = None,
-                  solver_name: str | None = None, extra: str = "", inits: str = ""):
+                  solver_name: str | None = None, extra: str = "", inits: str = "", boundary: str | None = None):
     """Runs the reference build for `steps` steps from the given initial fields
     (plane layout; missing components are zero) and returns
     ({name: plane-layout array}, timing dict).  With binary=REF_BIN_GPU and a
@@ -321,7 +324,8 @@ def run_reference(cfg: abi.Config, steps: int, init_fields: dict | None = None,
                 f.write(np.ascontiguousarray(full).tobytes())
     setup = os.path.join(tmp, "setup.dat")
     with open(setup, "w") as f:
-        f.write(setup_text(cfg, steps, init_path, solver_name=solver_name, extra=extra, inits=inits))
+        f.write(setup_text(cfg, steps, init_path, solver_name=solver_name, extra=extra, inits=inits,
+                           boundary=boundary))
     r = subprocess.run([binary, setup, tmp, *names], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"reference failed ({r.returncode}): {r.stderr[-2000:]}")

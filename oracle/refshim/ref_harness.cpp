@@ -16,6 +16,15 @@
 //  3. Output: after the run every full-size grid named on the command line is
 //     written as raw doubles (C order, ghost cells included), and the wall time
 //     of the step loop alone is printed as one JSON line.
+//  4. "slab_xy_periodic { z0 Z0 z1 Z1 }": the single_xy_periodic boundary
+//     (periodic_bound.cpp:87-130) over the z-planes Z0..Z1 of the global grid
+//     only (plus one ghost plane each side), the slab one process of MPulse's
+//     z-split MPI run holds (mpi_bound.cpp:66-109), with no halo exchange.
+//     Storage::getBorderExtent (storage.cpp:208-318) then gives the CPML faces
+//     and the injection plane only to the slabs that contain them, so a set
+//     of slab processes does the per-cell work of the whole grid; used to time
+//     the reference on the host cores (the fields at slab edges are not those
+//     of the whole grid).
 //
 // Usage: mpulse_ref SETUP OUTDIR [grid names...]
 // Environment: MPULSE_REF_WARMUP=W times only the steps after the first W.
@@ -43,6 +52,8 @@
 #include "diagnostic.h"
 #include "fdtd_plrc.h"
 #include "init.h"
+#include "periodic_bound.h"
+#include "globals.h"
 #undef private
 #undef protected
 
@@ -120,6 +131,29 @@ void MaskedCore<FDTD_PLRCNonlinCore>::callBase(double dt, int i, int j, int k, d
   this->chi = chiSave;
 }
 
+class SlabXYPeriodicBoundary : public SingleXYPeriodicBoundary {
+ public:
+  int z0 = 1, z1 = 1;
+  GridIndex lo, hi;
+  void init() {
+    lo = Globals::instance().gridLow();
+    hi = Globals::instance().gridHigh();
+    const int g0 = lo[2], g1 = hi[2];
+    lo[2] = std::max(g0, z0 - 1);
+    hi[2] = std::min(g1, z1 + 1);
+  }
+  const GridIndex &RegionLow() const { return lo; }
+  const GridIndex &RegionHigh() const { return hi; }
+
+ protected:
+  ParameterMap *MakeParamMap(ParameterMap *pm) {
+    pm = Rebuildable::MakeParamMap(pm);
+    (*pm)["z0"] = WParameter(new ParameterValue<int>(&z0, 1));
+    (*pm)["z1"] = WParameter(new ParameterValue<int>(&z1, 1));
+    return pm;
+  }
+};
+
 typedef FDTD_PLRCSolver<MaskedCore<FDTD_PLRCLinCore> > MaskedLin;
 typedef FDTD_PLRCSolver<MaskedCore<FDTD_PLRCNonlinCore> > MaskedNonlin;
 
@@ -162,6 +196,8 @@ class HarnessFieldSim : public FieldSimulation {
         WParameter(new ParameterRebuild<MaskedNonlin, FieldSolver>(&solver));
     (*pm)["raw_init"] =
         WParameter(new ParameterRebuild<RawInit, FieldSimInit>(&initializers));
+    (*pm)["slab_xy_periodic"] =
+        WParameter(new ParameterRebuild<SlabXYPeriodicBoundary, Boundary>(&boundary));
 #ifdef MPB_WITH_GPU
     registerGpuSolvers(pm, &solver);
 #endif

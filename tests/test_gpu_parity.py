@@ -249,3 +249,37 @@ def test_save_and_load_state_resumes_bit_for_bit(case):
     with runtime.Simulation(other) as h:
         with pytest.raises(runtime.MPulseError):
             h.load_state(snap)
+
+
+@pytest.mark.parametrize("case", ["nonlin_all_short", "nonlin_odd_sizes", "nl_xy", "tma_nonlin_all_short",
+                                  "lin_split_cpmlz_gauss"])
+def test_kerr_counts(case):
+    """mp_kerr_counts: on seeded fields that are non-zero everywhere, every
+    medium cell of every E half-step runs the Newton solve once (PLRC-nonlin:
+    planes 1..nz inside the medium; fdtd-nl: planes 1..nz+1), each with 1 to
+    newton_max_iter iterations; the read resets the counters; the linear
+    solver counts nothing."""
+    cfg = make_case(case, abi.MP_FP64)
+    if case.startswith("tma"):
+        cfg.staging = abi.MP_STAGING_TMA
+    init = random_fields(cfg, seed=23, smooth=True)
+    steps = 3
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        g.kerr_counts()
+        g.step(steps)
+        solves, iters = g.kerr_counts()
+        assert g.kerr_counts() == (0, 0)
+    plane = cfg.nx * cfg.ny
+    if cfg.solver == abi.MP_SOLVER_NL:
+        want = steps * plane * (cfg.nz + 1)
+    elif cfg.solver == abi.MP_SOLVER_PLRC_NONLIN:
+        z0, z1 = max(cfg.medium_z0, 1), min(cfg.medium_z1, cfg.nz)
+        want = steps * plane * (z1 - z0 + 1)
+    else:
+        want = 0
+    assert solves == want
+    assert want <= iters <= want * cfg.newton_max_iter
+    if want:
+        assert iters > solves  # the solve from |E^n| takes more than one iteration where E changes

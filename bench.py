@@ -226,18 +226,31 @@ class PairRun:
                 self.record()
 
     def summary(self) -> dict:
+        """The error of the FP32 form is measured against the FP64 form's field
+        norm at its largest over the run (the pulse in the domain): late in the
+        run the pulse has left through the CPML and the field that remains is
+        a residue of 1e-4 of that norm, so its own relative error measures
+        rounding noise on the residue, not the field.  Both are reported; the
+        rel-L2 <= 1e-5 bar applies to the error over the peak norm and to the
+        relative error while the field norm is at least 1% of its peak."""
         recs = [r for r in self.records if r["norm"] > 0]
         peak = max(recs, key=lambda r: r["norm"])
         last = self.records[-1]
+        live = [r for r in recs if r["norm"] >= 0.01 * peak["norm"]]
         return {
             "steps": last["step"], "record_every": RECORD_EVERY,
-            "rel_l2_fp32_vs_fp64_final": last["rel_l2"],
-            "rel_l2_fp32_vs_fp64_max": max(r["rel_l2"] for r in recs),
-            "rel_l2_fp32_vs_fp64_at_peak_norm": peak["rel_l2"], "peak_norm_step": peak["step"],
+            "error_over_peak_norm_max": max(r["err"] for r in self.records) / peak["norm"],
             "final_error_over_peak_norm": last["err"] / peak["norm"],
+            "rel_l2_fp32_vs_fp64_max_while_norm_ge_1pct_of_peak": max(r["rel_l2"] for r in live),
+            "steps_with_norm_ge_1pct_of_peak": [live[0]["step"], live[-1]["step"]],
+            "rel_l2_fp32_vs_fp64_at_peak_norm": peak["rel_l2"], "peak_norm_step": peak["step"],
+            "rel_l2_fp32_vs_fp64_final": last["rel_l2"],
             "final_norm_over_peak_norm": last["norm"] / peak["norm"],
+            "rel_l2_trace": [[r["step"], r["rel_l2"], r["norm"] / peak["norm"]] for r in self.records],
             "followmax": {"field": "Ex", "dim": "z", "line_xy": list(self.axis), "every_step": True,
                           "start_z": self.start,
+                          "max_abs_diff_cells_while_norm_ge_1pct_of_peak":
+                              max(abs(r["follow32"] - r["follow64"]) for r in live),
                           "max_abs_diff_cells": max(abs(r["follow32"] - r["follow64"]) for r in self.records),
                           "trace": [[r["step"], round(r["follow32"], 4), round(r["follow64"], 4)]
                                     for r in self.records]},
@@ -774,6 +787,8 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only mp_objective + mp_adjoint of the adjoint workload for --steps steps (ncu captures)")
     ap.add_argument("--checkpoint", type=int, default=50, help="checkpoint interval of --adjoint-only")
+    ap.add_argument("--adjoint-ratio", action="store_true",
+                    help="only the adjoint workload's wall-time ratios (the `adjoint` object of the bench line)")
     ap.add_argument("--adjoint-large", action="store_true",
                     help="the 512x512x768 nonlinear adjoint workload for --steps steps (minutes)")
     ap.add_argument("--budget-gb", type=float, default=120.0, help="checkpoint budget of --adjoint-large")
@@ -782,7 +797,9 @@ def main():
         args.warmup = 3
     if args.nz:
         WORKLOAD["nz"] = args.nz
-    if args.adjoint_large:
+    if args.adjoint_ratio:
+        out = run_adjoint(0)
+    elif args.adjoint_large:
         out = run_adjoint_large(args)
     elif args.adjoint_only:
         out = run_adjoint_profile(args)

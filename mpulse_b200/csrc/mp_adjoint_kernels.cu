@@ -19,10 +19,15 @@
 //     advances its E-face totals;
 //   adj_b_kernel (B cells, planes 0..nz)  gathers the adjoint of B from G
 //     through the transposed curl_E and the E-face totals, adds the
-//     objective's B term and advances its H-face totals.
+//     objective's B term and advances its H-face totals;
+//   adj_grad_kernel (design cells only)  accumulates the design gradients of
+//     the step from G, E before and after the step and the PLRC accumulator
+//     adjoints adj_e saved for the design cells; it runs on a second stream
+//     beside adj_b, so that adj_e, which every cell runs, carries none of the
+//     FP64 gradient arithmetic.
 // The Kerr linearisation and the gradient accumulation are FP64; the rest is
-// in the precision of the forward state.  Memory-bound; one thread per (x, y)
-// column and chunk of planes.
+// in the precision of the forward state.  Latency-bound at small grids; one
+// thread per (x, y) column and chunk of planes.
 #include "mp_checked.cuh"
 #include "mp_device.h"
 
@@ -250,18 +255,16 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
         ne[c] = p.eps_bg_t * g[c];
       }
     } else {
-      const double dD = p.sumChi0 - p.sumXi0;
-      double denom = 0.0, A = p.A0;
+      double A = p.A0;
       R idn = p.inv_denom0_t, numer = p.numer0_t, Rchi = p.chi_nl_t;
       if (dcell) {
-        denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
+        const double denom = d.lin ? e + s * (p.sumChi0 - p.sumXi0) : e + s * p.sumChi0 - s * p.sumXi0;
         A = p.nonlin ? u * p.chi / denom : 0.0;
         idn = R(1.0 / denom);
         numer = R(e - s * p.sumXi0);
         Rchi = R(p.nonlin ? u * p.chi : 0.0);
       }
       R cb[3] = {a[0], a[1], a[2]};
-      double Abar = 0.0;
       if (plrc_nl) {
         // E' = r c/|c| with r + A r^3 = |c|: dE'/dc = (I - e e^T) / (1 + A r^2)
         // + e e^T / (1 + 3 A r^2), dr/dA = -r^3 / (1 + 3 A r^2), c = E' (1 + A r^2)
@@ -277,7 +280,6 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) cb[c] = R(al * (a[c] - eh[c] * ea) + be * eh[c] * ea);
-        Abar = -ea * r * r2 * be;
       }
       const R E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
 #pragma unroll
@@ -286,8 +288,19 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
       const R f = numer + Rchi * E2;
 #pragma unroll
       for (int c = 0; c < 3; ++c) ne[c] = f * g[c] + R(2) * Rchi * En[c] * Eg;
+      // the design cells' accumulator adjoints before the reverse recursion,
+      // for adj_grad
+      if (dcell) {
+#pragma unroll
+        for (int n = 0; n < NP; ++n)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const long long q = ((di * NP + n) * 3 + c) * 2;
+            st_c(p.dpsi, q, p.n_design * NP * 6, st, T(pq[n][c][0]));
+            st_c(p.dpsi, q + 1, p.n_design * NP * 6, st, T(pq[n][c][1]));
+          }
+      }
       // reverse PLRC recursion: psi~bar = conj(Crec) psibar + g
-      double gs = 0.0;
       const R Rs = dcell ? R(s) : R(1);
 #pragma unroll
       for (int n = 0; n < NP; ++n) {
@@ -300,37 +313,9 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
           const R tr = Cr * pr + Ci * pim + g[c];
           const R ti = Cr * pim - Ci * pr;
           ne[c] += Rs * (Dr * tr + Di * ti + Xr * pr + Xi * pim);
-          if (dcell) {
-            const double CDr = p.pC[n][0] * p.pD[n][0] - p.pC[n][1] * p.pD[n][1];
-            const double CDi = p.pC[n][0] * p.pD[n][1] + p.pC[n][1] * p.pD[n][0];
-            gs += ((double)pr * (p.pxi[n][0] + CDr) + (double)pim * (p.pxi[n][1] + CDi)) * (double)En[c];
-          }
           pq[n][c][0] = tr;
           pq[n][c][1] = ti;
         }
-      }
-      if (dcell) {
-        double SD = 0.0;
-#pragma unroll
-        for (int n = 0; n < NP; ++n) SD += p.pD[n][0];
-        double ge = -Abar * A / denom, gu = 0.0;
-        gs -= Abar * A * dD / denom;
-        // c = E' (1 + A |E'|^2); A = 0 in the linear case
-        const double grow = 1.0 + A * ((double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const double cv = (double)En1[c] * grow;
-          ge += (double)g[c] * ((double)En[c] - cv);
-          gs += (double)g[c] * ((SD - p.sumXi0) * (double)En[c] - cv * dD);
-        }
-        if (p.nonlin) {
-          gu = Abar * p.chi / denom;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) gu += (double)g[c] * p.chi * (double)E2 * (double)En[c];
-        }
-        st_c(p.grad[0], di, p.n_design, st, ld_c(p.grad[0], di, p.n_design, st) + ge);
-        st_c(p.grad[1], di, p.n_design, st, ld_c(p.grad[1], di, p.n_design, st) + gs);
-        st_c(p.grad[2], di, p.n_design, st, ld_c(p.grad[2], di, p.n_design, st) + gu);
       }
     }
     // the objective's E term of the state before the step
@@ -381,6 +366,85 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     bx_km = bx;
     by_km = by;
   }
+}
+
+// The design gradients of one step, one thread per design cell (the design
+// box lies inside the medium planes and the interior).  From the E half
+// X = (numer + chi |E|^2) E + dt (curl + J) + Re sum psi~ with numer = e - s
+// sumXi0, denom = e + s (sumChi0 - sumXi0), psi~ = s (dchi0 - dxi0) E + psi,
+// psi' = s dxi0 E + Crec psi~ and (nonlinear) A = u chi / denom, with g the
+// adjoint of X / denom that adj_e stored in G:
+//   dJ/de += g . (E - c) - Abar A / denom
+//   dJ/ds += sum_n,c psibar_nc . (dxi0 + Crec (dchi0 - dxi0)) E_c
+//            + g . ((sum_n Re(dchi0 - dxi0) - sumXi0) E - c dD) - Abar A dD / denom
+//   dJ/du += g . chi |E|^2 E + Abar chi / denom
+// where c = E' (1 + A |E'|^2) is X / denom, dD = sumChi0 - sumXi0 and Abar,
+// the adjoint of A through the Kerr solve, is -(e^ . c_bar) r^3 with r = |E'|,
+// e^ = E' / r and c_bar = g denom the adjoint of c (the Kerr linearisation of
+// adj_e gives e^ . c_bar = be (e^ . a) with be = 1 / (1 + 3 A r^2)).
+template <typename T, int NP>
+__global__ void __launch_bounds__(MPB_ADJ_THREADS) adj_grad_kernel(const AdjParams<T> p) {
+  const DesignParams &d = p.design;
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kk = blockIdx.z;
+  if (ii >= d.bx || jj >= d.by) return;
+  const int i = d.x0 + ii, j = d.y0 + jj, k = d.z0 + kk;
+  const long long nf = p.n_field;
+  int *const st = p.status;
+  const long long di = ((long long)kk * d.by + jj) * d.bx + ii;
+  const long long c0 = (long long)k * p.plane + (long long)j * p.nx + i;
+  const double e = ld_c(d.eps, di, p.n_design, st), s = ld_c(d.dscale, di, p.n_design, st),
+               u = ld_c(d.chiscale, di, p.n_design, st);
+  T g[3], En[3], En1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    g[c] = ld_c(p.G[c], c0, nf, st);
+    En[c] = ld_c(p.En[c], c0, nf, st);
+    En1[c] = ld_c(p.En1[c], c0, nf, st);
+  }
+  const double dD = p.sumChi0 - p.sumXi0;
+  const double denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
+  const double A = p.nonlin ? u * p.chi / denom : 0.0;
+  const double r2 = (double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2];
+  double Abar = 0.0;
+  if (p.nonlin && r2 > 0) {
+    const double r = sqrt(r2);
+    double ecb = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ecb += (double)En1[c] / r * ((double)g[c] * denom);
+    Abar = -ecb * r * r2;
+  }
+  const T E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
+  double gs = 0.0, SD = 0.0;
+#pragma unroll
+  for (int n = 0; n < NP; ++n) {
+    SD += p.pD[n][0];
+    const double CDr = p.pC[n][0] * p.pD[n][0] - p.pC[n][1] * p.pD[n][1];
+    const double CDi = p.pC[n][0] * p.pD[n][1] + p.pC[n][1] * p.pD[n][0];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long q = ((di * NP + n) * 3 + c) * 2;
+      const double pr = ld_c(p.dpsi, q, p.n_design * NP * 6, st), pim = ld_c(p.dpsi, q + 1, p.n_design * NP * 6, st);
+      gs += (pr * (p.pxi[n][0] + CDr) + pim * (p.pxi[n][1] + CDi)) * (double)En[c];
+    }
+  }
+  double ge = -Abar * A / denom, gu = 0.0;
+  gs -= Abar * A * dD / denom;
+  const double grow = 1.0 + A * r2;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double cv = (double)En1[c] * grow;
+    ge += (double)g[c] * ((double)En[c] - cv);
+    gs += (double)g[c] * ((SD - p.sumXi0) * (double)En[c] - cv * dD);
+  }
+  if (p.nonlin) {
+    gu = Abar * p.chi / denom;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gu += (double)g[c] * p.chi * (double)E2 * (double)En[c];
+  }
+  st_c(p.grad[0], di, p.n_design, st, ld_c(p.grad[0], di, p.n_design, st) + ge);
+  st_c(p.grad[1], di, p.n_design, st, ld_c(p.grad[1], di, p.n_design, st) + gs);
+  st_c(p.grad[2], di, p.n_design, st, ld_c(p.grad[2], di, p.n_design, st) + gu);
 }
 
 template <typename T>
@@ -633,6 +697,20 @@ cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
 }
 
 template <typename T>
+cudaError_t launch_adj_grad(const AdjParams<T> &p, cudaStream_t st) {
+  const DesignParams &d = p.design;
+  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
+      g((d.bx + 31) / 32, (d.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, d.z1 - d.z0 + 1);
+  switch (p.np) {
+    case 0: adj_grad_kernel<T, 0><<<g, b, 0, st>>>(p); break;
+    case 1: adj_grad_kernel<T, 1><<<g, b, 0, st>>>(p); break;
+    case 2: adj_grad_kernel<T, 2><<<g, b, 0, st>>>(p); break;
+    default: adj_grad_kernel<T, 3><<<g, b, 0, st>>>(p); break;
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_adj_b(const AdjParams<T> &p, cudaStream_t st) {
   const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
       g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b);
@@ -662,6 +740,8 @@ cudaError_t launch_sum_terms(const double *terms, long long n, double *out, cuda
 
 template cudaError_t launch_adj_e<float>(const AdjParams<float> &, cudaStream_t);
 template cudaError_t launch_adj_e<double>(const AdjParams<double> &, cudaStream_t);
+template cudaError_t launch_adj_grad<float>(const AdjParams<float> &, cudaStream_t);
+template cudaError_t launch_adj_grad<double>(const AdjParams<double> &, cudaStream_t);
 template cudaError_t launch_adj_b<float>(const AdjParams<float> &, cudaStream_t);
 template cudaError_t launch_adj_b<double>(const AdjParams<double> &, cudaStream_t);
 template cudaError_t launch_adj_init<float>(const AdjParams<float> &, cudaStream_t);

@@ -43,7 +43,14 @@ cudaError_t launch_e_half_tma(const EParams<T> &, const ETmaMaps &, int, int, cu
 template <typename T>
 cudaError_t launch_b_half_tma(const BParams<T> &, const BTmaMaps &, cudaStream_t);
 void tma_boxes(int esz, int e_box[7][2], int b_box[6][2]);
+#ifndef MPB_ADJ_E_BPSM
+#define MPB_ADJ_E_BPSM 8
+#endif
+#ifndef MPB_ADJ_B_BPSM
+#define MPB_ADJ_B_BPSM 8
+#endif
 template <typename T> cudaError_t launch_adj_e(const AdjParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_adj_grad(const AdjParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_adj_b(const AdjParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_adj_init(const AdjParams<T> &, cudaStream_t);
 template <typename T>
@@ -315,6 +322,7 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
   bp.k_first = zper ? 1 : 0;
   bp.k_last = g.nz;
   ep.dt = bp.dt = T(g.dt);
+  ep.dt_lo = bp.dt_lo = T(g.dt - double(T(g.dt)));
   ep.mz0 = c->mz0;
   ep.mz1 = c->mz1;
   for (int s = 0; s < c->np; ++s)
@@ -327,6 +335,8 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
     }
   ep.numer = T(numer);
   ep.inv_denom = T(1.0 / denom);
+  ep.numer_lo = T(numer - double(ep.numer));
+  ep.inv_denom_lo = T(1.0 / denom - double(ep.inv_denom));
   ep.eps_bg = T(g.eps_bg);
   ep.inv_eps_bg = T(1.0 / g.eps_bg);
   ep.chi_over_denom = g.chi / denom;
@@ -1636,27 +1646,38 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   // The reverse pass runs on a second stream: the adjoint kernels of one chunk
   // overlap the forward run of the next, which only shares the history buffer
   // the chunk reads (events order the two).
+  // The design gradients of each reverse step run on a third stream beside
+  // adj_b (adj_grad reads what adj_e wrote and must finish before the next
+  // adj_e overwrites it).
   struct RevStream {
-    cudaStream_t s = nullptr;
+    cudaStream_t s = nullptr, g = nullptr;
     cudaEvent_t fwd[2] = {nullptr, nullptr}, rev[2] = {nullptr, nullptr};
+    cudaEvent_t e_done = nullptr, g_done = nullptr;
     bool used[2] = {false, false};
     ~RevStream() {
-      if (s) {
-        cudaStreamSynchronize(s);
-        cudaStreamDestroy(s);
-      }
+      for (cudaStream_t q : {s, g})
+        if (q) {
+          cudaStreamSynchronize(q);
+          cudaStreamDestroy(q);
+        }
       for (int q = 0; q < 2; ++q) {
         if (fwd[q]) cudaEventDestroy(fwd[q]);
         if (rev[q]) cudaEventDestroy(rev[q]);
       }
+      if (e_done) cudaEventDestroy(e_done);
+      if (g_done) cudaEventDestroy(g_done);
     }
   } rs;
-  if ((e = cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&rs.g, cudaStreamNonBlocking)) != cudaSuccess)
     return cuda_err(c, e, "cudaStreamCreate");
   for (int q = 0; q < 2; ++q)
     if ((e = cudaEventCreateWithFlags(&rs.fwd[q], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&rs.rev[q], cudaEventDisableTiming)) != cudaSuccess)
       return cuda_err(c, e, "cudaEventCreate");
+  if ((e = cudaEventCreateWithFlags(&rs.e_done, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&rs.g_done, cudaEventDisableTiming)) != cudaSuccess)
+    return cuda_err(c, e, "cudaEventCreate");
   int cur = 0;  // history buffer of the chunk being run forward
   AdjParams<T> p = AdjParams<T>();
   for (int q = 0; q < 3; ++q) {
@@ -1677,6 +1698,12 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       if ((e = buf.alloc(&ps, 2 * c->psi_cells * sizeof(T))) != cudaSuccess) return cuda_err(c, e, "adjoint allocation");
       p.psib[s][q] = static_cast<T *>(ps);
     }
+  {
+    void *dp = nullptr;
+    if (c->np > 0 && (e = buf.alloc(&dp, c->dcells * c->np * 6 * sizeof(T))) != cudaSuccess)
+      return cuda_err(c, e, "adjoint allocation");
+    p.dpsi = static_cast<T *>(dp);
+  }
   for (int isH = 0; isH < 2; ++isH) {
     const int rc = adj_faces<T>(c, buf, isH != 0, isH ? bp.cpml : ep.cpml, isH ? p.fh : p.fe);
     if (rc != MP_OK) return rc;
@@ -1687,11 +1714,14 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   p.n_psi = (long long)c->psi_cells;
   p.n_design = (long long)c->dcells;
   {
-    // planes per block: enough blocks to fill 148 SMs several times over
-    const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
-    const long long chunks = std::max(1LL, (148LL * 8 + blocks_xy - 1) / blocks_xy);
-    p.kchunk_e = int(std::max(1LL, (g.nz + chunks - 1) / chunks));
-    p.kchunk_b = int(std::max(1LL, (g.nz + 1 + chunks - 1) / chunks));
+    // planes per block: about MPB_ADJ_E_BPSM / MPB_ADJ_B_BPSM blocks of 32 x 4
+    // columns per SM (measured on the 96^3 adjoint workload, FP32: for adj_e
+    // 6 planes per block beat 3 and 2)
+    const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 3) / 4);
+    const long long ce = std::max(1LL, (148LL * MPB_ADJ_E_BPSM + blocks_xy - 1) / blocks_xy);
+    const long long cb = std::max(1LL, (148LL * MPB_ADJ_B_BPSM + blocks_xy - 1) / blocks_xy);
+    p.kchunk_e = int(std::max(1LL, (g.nz + ce - 1) / ce));
+    p.kchunk_b = int(std::max(1LL, (g.nz + 1 + cb - 1) / cb));
 #ifdef MPB_ADJ_KCHUNK
     p.kchunk_e = p.kchunk_b = MPB_ADJ_KCHUNK;
 #endif
@@ -1858,8 +1888,14 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       p.oby = slot_b(n - n0, 1);
       p.add_obj = n >= 1;
       if ((err = launch_adj_e<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint E kernel");
+      if ((err = cudaEventRecord(rs.e_done, rs.s)) != cudaSuccess ||
+          (err = cudaStreamWaitEvent(rs.g, rs.e_done, 0)) != cudaSuccess)
+        return cuda_err(c, err, "event");
+      if ((err = launch_adj_grad<T>(p, rs.g)) != cudaSuccess) return cuda_err(c, err, "adjoint gradient kernel");
+      if ((err = cudaEventRecord(rs.g_done, rs.g)) != cudaSuccess) return cuda_err(c, err, "event");
       if ((err = launch_adj_b<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint B kernel");
-      c->launches += 2;
+      if ((err = cudaStreamWaitEvent(rs.s, rs.g_done, 0)) != cudaSuccess) return cuda_err(c, err, "event");
+      c->launches += 3;
     }
     if ((err = cudaEventRecord(rs.rev[cur], rs.s)) != cudaSuccess) return cuda_err(c, err, "event");
     rs.used[cur] = true;

@@ -141,6 +141,24 @@ __device__ __forceinline__ void flush_kerr_count(unsigned long long *dst, const 
   }
 }
 
+// dt * u with the FP32 form's compensated step (hi + lo): the exact product
+// dt * u plus dt_lo * u, rounded once.  FP64: dt * u.
+template <typename T>
+__device__ __forceinline__ T dt_mul(T dt, T dt_lo, T u) {
+  return sizeof(T) == 4 ? fma(dt, u, dt_lo * u) : dt * u;
+}
+
+// numer * e + a and x * inv_denom with the compensated coefficients of the
+// FP32 form; in FP64 the plain products.
+template <typename T>
+__device__ __forceinline__ T numer_mul_add(T numer, T numer_lo, T e, T a) {
+  return sizeof(T) == 4 ? fma(numer, e, fma(numer_lo, e, a)) : numer * e + a;
+}
+template <typename T>
+__device__ __forceinline__ T inv_denom_mul(T x, T idn, T idn_lo) {
+  return sizeof(T) == 4 ? fma(x, idn, x * idn_lo) : x * idn;
+}
+
 // Values one E update reads: B at the cell and its x-1, y-1, z-1 neighbours
 // (the ones the curl uses) and the old E.
 template <typename T>
@@ -172,6 +190,7 @@ struct BIn {
 template <typename T, int NP>
 struct CellCoef {
   T numer, inv_denom, chi;
+  T numer_lo, inv_denom_lo;  // FP32 form: the rounding errors of numer and inv_denom (zero in FP64)
   double chi_over_denom;
   T pD[NP > 0 ? NP : 1][2], pxi[NP > 0 ? NP : 1][2];
 };
@@ -180,6 +199,8 @@ template <typename T, int NP, bool DESIGN>
 __device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int k, bool med, CellCoef<T, NP> &cc) {
   cc.numer = p.numer;
   cc.inv_denom = p.inv_denom;
+  cc.numer_lo = p.numer_lo;
+  cc.inv_denom_lo = p.inv_denom_lo;
   cc.chi = p.chi;
   cc.chi_over_denom = p.chi_over_denom;
 #pragma unroll
@@ -195,8 +216,11 @@ __device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int
       const long long di = ((long long)(k - d.z0) * d.by + (j - d.y0)) * d.bx + (i - d.x0);
       const double e = d.eps[di], s = d.dscale[di], u = d.chiscale[di];
       const double denom = d.lin ? e + s * (d.sumChi0 - d.sumXi0) : e + s * d.sumChi0 - s * d.sumXi0;
-      cc.numer = T(e - s * d.sumXi0);
-      cc.inv_denom = T(1.0 / denom);
+      const double nm = e - s * d.sumXi0, idn = 1.0 / denom;
+      cc.numer = T(nm);
+      cc.inv_denom = T(idn);
+      cc.numer_lo = T(nm - double(cc.numer));
+      cc.inv_denom_lo = T(idn - double(cc.inv_denom));
       cc.chi = T(u * d.chi);
       cc.chi_over_denom = u * d.chi / denom;
 #pragma unroll
@@ -282,14 +306,16 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
   const T cbz = (v.by - v.by_xm) * ikx - (v.bx - v.bx_ym) * iky;
   const T ex = v.ex, ey = v.ey, ez = v.ez;
 
+  const T dtl = p.dt_lo;
   if (MODE == MODE_PLAIN) {
-    exn = ex + dt * cbx;
-    eyn = ey + dt * cby;
-    ezn = ez + dt * cbz;
+    exn = ex + dt_mul(dt, dtl, cbx);
+    eyn = ey + dt_mul(dt, dtl, cby);
+    ezn = ez + dt_mul(dt, dtl, cbz);
   } else if (MODE == MODE_NL) {
     const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
     const T f = T(p.eps_d + p.chi_d * E2);
-    const T Dx = f * ex + dt * cbx, Dy = f * ey + dt * cby, Dz = f * ez + dt * cbz;
+    const T Dx = f * ex + dt_mul(dt, dtl, cbx), Dy = f * ey + dt_mul(dt, dtl, cby),
+            Dz = f * ez + dt_mul(dt, dtl, cbz);
     const double D2 = (double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz;
     if (D2 > 0) {
       const double rD = rsqrt(D2);  // as in the PLRC Kerr update below
@@ -306,9 +332,9 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     }
   } else if (!med) {
     // background: no poles, no Kerr term
-    exn = (p.eps_bg * ex + dt * (cbx + jx)) * p.inv_eps_bg;
-    eyn = (p.eps_bg * ey + dt * (cby + jy)) * p.inv_eps_bg;
-    ezn = (p.eps_bg * ez + dt * (cbz + jz)) * p.inv_eps_bg;
+    exn = (p.eps_bg * ex + dt_mul(dt, dtl, cbx + jx)) * p.inv_eps_bg;
+    eyn = (p.eps_bg * ey + dt_mul(dt, dtl, cby + jy)) * p.inv_eps_bg;
+    ezn = (p.eps_bg * ez + dt_mul(dt, dtl, cbz + jz)) * p.inv_eps_bg;
   } else {
     T Px = T(0), Py = T(0), Pz = T(0);
     if (NP > 0) {
@@ -332,22 +358,50 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       Pz = P3[2];
     }
     if (MODE == MODE_PLRC_LIN) {
-      exn = (lc.numer * ex + (dt * (cbx + jx) + Px)) * lc.inv_denom;
-      eyn = (lc.numer * ey + (dt * (cby + jy) + Py)) * lc.inv_denom;
-      ezn = (lc.numer * ez + (dt * (cbz + jz) + Pz)) * lc.inv_denom;
+      exn = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ex, dt_mul(dt, dtl, cbx + jx) + Px), lc.inv_denom,
+                          lc.inv_denom_lo);
+      eyn = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ey, dt_mul(dt, dtl, cby + jy) + Py), lc.inv_denom,
+                          lc.inv_denom_lo);
+      ezn = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ez, dt_mul(dt, dtl, cbz + jz) + Pz), lc.inv_denom,
+                          lc.inv_denom_lo);
     } else {
       const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
       const T f = lc.numer + lc.chi * T(E2);
-      const T cx = (f * ex + dt * (cbx + jx) + Px) * lc.inv_denom;
-      const T cy = (f * ey + dt * (cby + jy) + Py) * lc.inv_denom;
-      const T cz = (f * ez + dt * (cbz + jz) + Pz) * lc.inv_denom;
+      T cx, cy, cz;
+      if (sizeof(T) == 4) {
+        // (numer + chi |E|^2) E + dt u + P with the compensated numer and dt
+        const T kf = lc.chi * T(E2);
+        cx = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ex, fma(kf, ex, dt_mul(dt, dtl, cbx + jx) + Px)),
+                           lc.inv_denom, lc.inv_denom_lo);
+        cy = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ey, fma(kf, ey, dt_mul(dt, dtl, cby + jy) + Py)),
+                           lc.inv_denom, lc.inv_denom_lo);
+        cz = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ez, fma(kf, ez, dt_mul(dt, dtl, cbz + jz) + Pz)),
+                           lc.inv_denom, lc.inv_denom_lo);
+      } else {
+        cx = (f * ex + dt * (cbx + jx) + Px) * lc.inv_denom;
+        cy = (f * ey + dt * (cby + jy) + Py) * lc.inv_denom;
+        cz = (f * ez + dt * (cbz + jz) + Pz) * lc.inv_denom;
+      }
       // |c|, 1/|c| and the start |E^n| from reciprocal square roots: no FP64
-      // square root or division here (equal to sqrt and / up to rounding)
+      // square root or division here (equal to sqrt and / up to rounding).
+      // The FP32 form takes 1/|c| from the single-precision estimate refined
+      // by one FP64 Newton-Raphson step r <- r (3/2 - C2 r^2 / 2) (relative
+      // error about 1e-14, far below the FP32 rounding of the result) and the
+      // start |E^n| of the Newton solve in single precision (the solve
+      // converges to the same root from any start near it); outside the
+      // normal single-precision range it takes the FP64 path.
       const double C2 = (double)cx * cx + (double)cy * cy + (double)cz * cz;
       if (C2 > 0) {
-        const double rC = rsqrt(C2);
+        double rC, E0;
+        if (sizeof(T) == 4 && C2 > 1e-30 && C2 < 1e30) {
+          rC = (double)rsqrtf((float)C2);
+          rC = rC * fma(-0.5 * C2, rC * rC, 1.5);
+          E0 = (double)sqrtf((float)E2);
+        } else {
+          rC = rsqrt(C2);
+          E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
+        }
         const double C = C2 * rC;
-        const double E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
         const double E = kerr_newton(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status, &kc.iters);
         ++kc.solves;
         const double sc = E * rC;
@@ -428,9 +482,9 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
   }
 
   // ---- plrcStepB (fdtd_plrc.cpp:263-293)
-  bxn = v.bx + dt * ((v.ey_kp - v.ey) * ikz - (v.ez_yp - v.ez) * iky + mx);
-  byn = v.by + dt * ((v.ez_xp - v.ez) * ikx - (v.ex_kp - v.ex) * ikz + my);
-  bzn = v.bz + dt * ((v.ex_yp - v.ex) * iky_bz - (v.ey_xp - v.ey) * ikx + mz);
+  bxn = v.bx + dt_mul(dt, p.dt_lo, (v.ey_kp - v.ey) * ikz - (v.ez_yp - v.ez) * iky + mx);
+  byn = v.by + dt_mul(dt, p.dt_lo, (v.ez_xp - v.ez) * ikx - (v.ex_kp - v.ex) * ikz + my);
+  bzn = v.bz + dt_mul(dt, p.dt_lo, (v.ex_yp - v.ex) * iky_bz - (v.ey_xp - v.ey) * ikx + mz);
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;

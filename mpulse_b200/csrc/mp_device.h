@@ -88,6 +88,11 @@ struct EParams {
   int zperiodic;
   int kchunk;             // planes per block
   T dt;
+  // FP32 form: the rounding error of dt, numer and inv_denom as floats
+  // (x - float(x)), so that the updates apply the FP64 coefficients (hi + lo)
+  // and the FP32 rounding of the coefficients does not add up step after
+  // step; zero in the FP64 form
+  T dt_lo, numer_lo, inv_denom_lo;
 
   // PLRC (fdtd_plrc.t:198-216), active poles only, in T; psi is complex
   // (re, im interleaved) over the medium planes mz0..mz1.
@@ -127,7 +132,7 @@ struct BParams {
   int k_first, k_last;    // 0..nz (xy periodic) or 1..nz (periodic)
   int zperiodic;
   int kchunk;
-  T dt;
+  T dt, dt_lo;            // dt_lo as in EParams
   const T *ik[3];         // 1 / (kappa_H * d)
   const T *ik_bz_y;       // line used for dEx/dy in the Bz update
   CpmlFace<T> cpml[6];
@@ -187,6 +192,9 @@ struct AdjParams {
   const T *obx, *oby;     // Bx, By of that state on the Sz plane (plane-sized)
   int *status;            // the context's status word
   long long n_field, n_psi, n_design;  // elements of a field array, pairs of a PLRC array, design cells
+  // the PLRC accumulator adjoints of the design cells before the step's E
+  // half, saved by adj_e for adj_grad: box-sized, [cell][pole][component][re, im]
+  T *dpsi;
 };
 
 // Field initialisers (mp_init_kernels.cu).

@@ -41,6 +41,13 @@
 #ifndef MPB_E_MIN_THREADS
 #define MPB_E_MIN_THREADS 768
 #endif
+// FP32 E half: resident threads per SM (the FP64 form keeps MPB_E_MIN_THREADS).
+// On the 256x256x512 workload with the pulse in the Kerr medium (FP32, where
+// the E half is latency- and issue-bound) 1024 threads (64 registers, 40 B
+// spilled) took the E half from 0.855 to 0.839 ms.
+#ifndef MPB_E_MIN_THREADS_F
+#define MPB_E_MIN_THREADS_F 1024
+#endif
 #ifndef MPB_B_MIN_THREADS
 #define MPB_B_MIN_THREADS 768
 #endif
@@ -76,7 +83,8 @@
 namespace mpb {
 
 template <typename T, int MODE, int NP, bool DESIGN>
-__global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y, MPB_E_MIN_THREADS / (32 * MPB_E_BLOCK_Y))
+__global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y,
+                                  (sizeof(T) == 4 ? MPB_E_MIN_THREADS_F : MPB_E_MIN_THREADS) / (32 * MPB_E_BLOCK_Y))
     e_half_kernel(const EParams<T> p) {
   typedef typename Vec2<T>::type T2;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based: MPulse i + 1
@@ -437,9 +445,9 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
     for (int c = 0; c < V; ++c) {
       const T ezx = c + 1 < V ? ez.v[c + 1 < V ? c + 1 : 0] : ez_xl;
       const T eyx = c + 1 < V ? ey.v[c + 1 < V ? c + 1 : 0] : ey_xl;
-      bxn.v[c] = bx.v[c] + dt * ((ey_kp.v[c] - ey.v[c]) * ikz - (ez_yp.v[c] - ez.v[c]) * iky + m[c][0]);
-      byn.v[c] = by.v[c] + dt * ((ezx - ez.v[c]) * ikx[c] - (ex_kp.v[c] - ex.v[c]) * ikz + m[c][1]);
-      bzn.v[c] = bz.v[c] + dt * ((ex_yp.v[c] - ex.v[c]) * iky_bz - (eyx - ey.v[c]) * ikx[c] + m[c][2]);
+      bxn.v[c] = bx.v[c] + dt_mul(dt, p.dt_lo, (ey_kp.v[c] - ey.v[c]) * ikz - (ez_yp.v[c] - ez.v[c]) * iky + m[c][0]);
+      byn.v[c] = by.v[c] + dt_mul(dt, p.dt_lo, (ezx - ez.v[c]) * ikx[c] - (ex_kp.v[c] - ex.v[c]) * ikz + m[c][1]);
+      bzn.v[c] = bz.v[c] + dt_mul(dt, p.dt_lo, (ex_yp.v[c] - ex.v[c]) * iky_bz - (eyx - ey.v[c]) * ikx[c] + m[c][2]);
     }
     stv_c(Bx, base + col, nf, st, bxn);
     stv_c(By, base + col, nf, st, byn);

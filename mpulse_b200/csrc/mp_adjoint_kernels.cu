@@ -20,11 +20,15 @@
 //   adj_b_kernel (B cells, planes 0..nz)  gathers the adjoint of B from G
 //     through the transposed curl_E and the E-face totals, adds the
 //     objective's B term and advances its H-face totals;
-//   adj_grad_kernel (design cells only)  accumulates the design gradients of
-//     the step from G, E before and after the step and the PLRC accumulator
-//     adjoints adj_e saved for the design cells; it runs on a second stream
-//     beside adj_b, so that adj_e, which every cell runs, carries none of the
-//     FP64 gradient arithmetic.
+//   the design gradients of the step (design cells only), accumulated from
+//     G, E before and after the step and the PLRC accumulator adjoints adj_e
+//     saved for the design cells, by extra blocks of the adj_b launch, so
+//     that adj_e, which every cell runs, carries none of the FP64 gradient
+//     arithmetic.
+// The kernels of the reverse pass are launched with programmatic dependent
+// launch: a kernel's blocks may start while the previous kernel's last blocks
+// run, do their set-up, and wait (griddepcontrol.wait) for the previous
+// kernel's writes before reading anything it produced.
 // The Kerr linearisation and the gradient accumulation are FP64; the rest is
 // in the precision of the forward state.  Latency-bound at small grids; one
 // thread per (x, y) column and chunk of planes.
@@ -99,15 +103,24 @@ __device__ __forceinline__ void face_w(const AdjFace<T> &F, int pos, int li, R c
   }
 }
 
+// Programmatic dependent launch: let the next kernel of the stream start its
+// blocks, and wait until the previous kernel's writes are visible.  Both are
+// no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace
 
 // Arithmetic is in T (the precision of the state); the Kerr linearisation and
 // the design gradients are FP64.  One thread per (x, y) column marches up a
-// chunk of planes, carrying the z-neighbours in registers.
+// chunk of planes, carrying the z-neighbours in registers.  Arrays a kernel
+// only reads (the B adjoint in adj_e, G in adj_b, the E history) go through
+// the read-only data path (ldg_c).
 template <typename T, int NP>
 __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_ADJ_E_MIN_D) / MPB_ADJ_THREADS)
     adj_e_kernel(const AdjParams<T> p) {
   typedef T R;
+  pdl_launch_dependents();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.nx || j >= p.ny) return;
@@ -134,6 +147,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   const bool warp_xy = __any_sync(__activemask(), (face_pos(HX, i + 1) >= 0) || (face_pos(HX, im + 1) >= 0) ||
                                                       (face_pos(HY, j + 1) >= 0) || (face_pos(HY, jm + 1) >= 0) ||
                                                       (face_pos(EX, i + 1) >= 0) || (face_pos(EY, j + 1) >= 0));
+  // everything below reads what the previous reverse kernel wrote
+  pdl_wait();
   // the z H face's c * total at plane k - 1, carried
   R cw0, cw1;
   bool cw_on;
@@ -145,8 +160,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   const DesignParams &d = p.design;
   const bool dxy = i >= d.x0 && i <= d.x1 && j >= d.y0 && j <= d.y1;
   const bool oxy = i >= p.ox0 && i <= p.ox1 && j >= p.oy0 && j <= p.oy1;
-  R bx_km = ld_c(Bx, (long long)(k0 - 1) * pl + col, nf, st);
-  R by_km = ld_c(By, (long long)(k0 - 1) * pl + col, nf, st);
+  R bx_km = ldg_c(Bx, (long long)(k0 - 1) * pl + col, nf, st);
+  R by_km = ldg_c(By, (long long)(k0 - 1) * pl + col, nf, st);
 
   const bool plrc_nl = p.nonlin != 0;
   for (int k = k0; k <= k1; ++k) {
@@ -155,16 +170,16 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
     const bool med = k >= p.mz0 && k <= p.mz1;
     const bool dcell = med && dxy && k >= d.z0 && k <= d.z1;
     // ---- every load of this plane first, so that their latencies overlap
-    const R bx = ld_c(Bx, c0, nf, st), by = ld_c(By, c0, nf, st), bz = ld_c(Bz, c0, nf, st);
-    const R bx_ym = ld_c(Bx, base + colym, nf, st), by_xm = ld_c(By, base + colxm, nf, st),
-            bz_ym = ld_c(Bz, base + colym, nf, st), bz_xm = ld_c(Bz, base + colxm, nf, st);
+    const R bx = ldg_c(Bx, c0, nf, st), by = ldg_c(By, c0, nf, st), bz = ldg_c(Bz, c0, nf, st);
+    const R bx_ym = ldg_c(Bx, base + colym, nf, st), by_xm = ldg_c(By, base + colxm, nf, st),
+            bz_ym = ldg_c(Bz, base + colym, nf, st), bz_xm = ldg_c(Bz, base + colxm, nf, st);
     const R kzk = p.ikH[2][k], kzm = p.ikH[2][k - 1];
     R a[3] = {R(ld_c(p.Eb[0], c0, nf, st)), R(ld_c(p.Eb[1], c0, nf, st)), R(ld_c(p.Eb[2], c0, nf, st))};
-    const R En[3] = {R(ld_c(p.En[0], c0, nf, st)), R(ld_c(p.En[1], c0, nf, st)), R(ld_c(p.En[2], c0, nf, st))};
+    const R En[3] = {R(ldg_c(p.En[0], c0, nf, st)), R(ldg_c(p.En[1], c0, nf, st)), R(ldg_c(p.En[2], c0, nf, st))};
     R En1[3] = {R(0), R(0), R(0)};
     if (med && (plrc_nl || dcell)) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) En1[c] = R(ld_c(p.En1[c], c0, nf, st));
+      for (int c = 0; c < 3; ++c) En1[c] = R(ldg_c(p.En1[c], c0, nf, st));
     }
     const long long pi = ((long long)(k - p.mz0) * ny + j) * nx + i;
     R pq[NP > 0 ? NP : 1][3][2];
@@ -383,11 +398,11 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
 // e^ = E' / r and c_bar = g denom the adjoint of c (the Kerr linearisation of
 // adj_e gives e^ . c_bar = be (e^ . a) with be = 1 / (1 + 3 A r^2)).
 template <typename T, int NP>
-__global__ void __launch_bounds__(MPB_ADJ_THREADS) adj_grad_kernel(const AdjParams<T> p) {
+__device__ __forceinline__ void adj_grad_cells(const AdjParams<T> &p, int gbx, int gby, int kk) {
   const DesignParams &d = p.design;
-  const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y * blockDim.y + threadIdx.y;
-  const int kk = blockIdx.z;
+  const int ii = gbx * blockDim.x + threadIdx.x, jj = gby * blockDim.y + threadIdx.y;
   if (ii >= d.bx || jj >= d.by) return;
+  pdl_wait();
   const int i = d.x0 + ii, j = d.y0 + jj, k = d.z0 + kk;
   const long long nf = p.n_field;
   int *const st = p.status;
@@ -399,8 +414,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS) adj_grad_kernel(const AdjPara
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     g[c] = ld_c(p.G[c], c0, nf, st);
-    En[c] = ld_c(p.En[c], c0, nf, st);
-    En1[c] = ld_c(p.En1[c], c0, nf, st);
+    En[c] = ldg_c(p.En[c], c0, nf, st);
+    En1[c] = ldg_c(p.En1[c], c0, nf, st);
   }
   const double dD = p.sumChi0 - p.sumXi0;
   const double denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
@@ -448,13 +463,12 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS) adj_grad_kernel(const AdjPara
 }
 
 template <typename T>
-__global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D) / MPB_ADJ_THREADS)
-    adj_b_kernel(const AdjParams<T> p) {
+__device__ __forceinline__ void adj_b_cells(const AdjParams<T> &p, int bxi, int byi, int bzi) {
   typedef T R;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = bxi * blockDim.x + threadIdx.x;
+  const int j = byi * blockDim.y + threadIdx.y;
   if (i >= p.nx || j >= p.ny) return;
-  const int k0 = blockIdx.z * p.kchunk_b;
+  const int k0 = bzi * p.kchunk_b;
   const int k1 = min(k0 + p.kchunk_b - 1, p.nz);
   if (k0 > k1) return;
   const int nx = p.nx, ny = p.ny;
@@ -486,8 +500,10 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
   // outside the z faces
   const bool warp_xy =
       __any_sync(__activemask(), (exo >= 0) || (exp_ >= 0) || (eyo >= 0) || (eyp >= 0) || (hxo >= 0) || (hyo >= 0));
+  // everything below reads what adj_e wrote
+  pdl_wait();
   // G and the z E face's c * total at plane k, carried from the previous plane's k + 1
-  R gx_k = ld_c(gx, (long long)k0 * pl + col, nf, st), gy_k = ld_c(gy, (long long)k0 * pl + col, nf, st);
+  R gx_k = ldg_c(gx, (long long)k0 * pl + col, nf, st), gy_k = ldg_c(gy, (long long)k0 * pl + col, nf, st);
   R zw0, zw1;
   bool zw_on;
   {
@@ -500,10 +516,10 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     const long long base = (long long)k * pl;
     const long long c0 = base + col;
     // ---- every load of this plane first
-    const R gx_kp = ld_c(gx, c0 + pl, nf, st), gy_kp = ld_c(gy, c0 + pl, nf, st);
-    const R gzk = ld_c(gz, c0, nf, st);
-    const R gx_yp = ld_c(gx, base + colyp, nf, st), gy_xp = ld_c(gy, base + colxp, nf, st),
-            gz_xp = ld_c(gz, base + colxp, nf, st), gz_yp = ld_c(gz, base + colyp, nf, st);
+    const R gx_kp = ldg_c(gx, c0 + pl, nf, st), gy_kp = ldg_c(gy, c0 + pl, nf, st);
+    const R gzk = ldg_c(gz, c0, nf, st);
+    const R gx_yp = ldg_c(gx, base + colyp, nf, st), gy_xp = ldg_c(gy, base + colxp, nf, st),
+            gz_xp = ldg_c(gz, base + colxp, nf, st), gz_yp = ldg_c(gz, base + colyp, nf, st);
     const R kzk = p.ikE[2][k], kzp = p.ikE[2][k + 1];
     R b[3] = {R(ld_c(p.Bb[0], c0, nf, st)), R(ld_c(p.Bb[1], c0, nf, st)), R(ld_c(p.Bb[2], c0, nf, st))};
     // faces on warps and planes that touch one: E faces (x / y hold planes
@@ -534,8 +550,8 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     const bool obj = oxy && k == p.oz0;
     R oex = R(0), oey = R(0);
     if (obj) {
-      oex = ld_c(p.En[0], c0, nf, st);
-      oey = ld_c(p.En[1], c0, nf, st);
+      oex = ldg_c(p.En[0], c0, nf, st);
+      oey = ldg_c(p.En[1], c0, nf, st);
     }
 
     // ---- transposed curl_E and E faces
@@ -586,6 +602,24 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
     }
     gx_k = gx_kp;
     gy_k = gy_kp;
+  }
+}
+
+// The B half of the reverse step (blocks 0 .. nb-1 of a one-dimensional grid,
+// x fastest over gx x gy x z-chunks) and the design gradients of the step
+// (the blocks after them, over the design box in 32 x 4 tiles, one plane
+// each).
+template <typename T, int NP>
+__global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D) / MPB_ADJ_THREADS)
+    adj_b_kernel(const AdjParams<T> p, const int gx, const int gy, const int nb) {
+  pdl_launch_dependents();
+  const int b = blockIdx.x;
+  if (b < nb) {
+    adj_b_cells<T>(p, b % gx, (b / gx) % gy, b / (gx * gy));
+  } else {
+    const int q = b - nb;
+    const int tx = (p.design.bx + 31) / 32, ty = (p.design.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y;
+    adj_grad_cells<T, NP>(p, q % tx, (q / tx) % ty, q / (tx * ty));
   }
 }
 
@@ -683,39 +717,53 @@ __global__ void __launch_bounds__(256) sum_terms_kernel(const double *terms, lon
 // ---------------------------------------------------------------------------
 // Launchers
 
+// A launch with programmatic stream serialisation (the kernel's blocks may
+// start before the previous kernel in the stream has finished; the kernel
+// orders its reads with griddepcontrol.wait).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 g, dim3 b, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <typename T>
 cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
   const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
       g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + p.kchunk_e - 1) / p.kchunk_e);
   switch (p.np) {
-    case 0: adj_e_kernel<T, 0><<<g, b, 0, st>>>(p); break;
-    case 1: adj_e_kernel<T, 1><<<g, b, 0, st>>>(p); break;
-    case 2: adj_e_kernel<T, 2><<<g, b, 0, st>>>(p); break;
-    default: adj_e_kernel<T, 3><<<g, b, 0, st>>>(p); break;
+    case 0: return launch_pdl(adj_e_kernel<T, 0>, g, b, st, p);
+    case 1: return launch_pdl(adj_e_kernel<T, 1>, g, b, st, p);
+    case 2: return launch_pdl(adj_e_kernel<T, 2>, g, b, st, p);
+    default: return launch_pdl(adj_e_kernel<T, 3>, g, b, st, p);
   }
-  return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_adj_grad(const AdjParams<T> &p, cudaStream_t st) {
-  const DesignParams &d = p.design;
-  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
-      g((d.bx + 31) / 32, (d.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, d.z1 - d.z0 + 1);
-  switch (p.np) {
-    case 0: adj_grad_kernel<T, 0><<<g, b, 0, st>>>(p); break;
-    case 1: adj_grad_kernel<T, 1><<<g, b, 0, st>>>(p); break;
-    case 2: adj_grad_kernel<T, 2><<<g, b, 0, st>>>(p); break;
-    default: adj_grad_kernel<T, 3><<<g, b, 0, st>>>(p); break;
-  }
-  return cudaGetLastError();
-}
-
+// adj_b of the step, with the design gradients (when there is a design box) in
+// extra blocks of the same launch.
 template <typename T>
 cudaError_t launch_adj_b(const AdjParams<T> &p, cudaStream_t st) {
-  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
-      g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b);
-  adj_b_kernel<T><<<g, b, 0, st>>>(p);
-  return cudaGetLastError();
+  const int gx = (p.nx + 31) / 32, gy = (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y,
+            gz = (p.nz + 1 + p.kchunk_b - 1) / p.kchunk_b;
+  const int nb = gx * gy * gz;
+  const DesignParams &d = p.design;
+  const int ng = d.x0 <= d.x1 ? ((d.bx + 31) / 32) * ((d.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y) * (d.z1 - d.z0 + 1)
+                              : 0;
+  const dim3 b(32, MPB_ADJ_BLOCK_Y, 1), g(nb + ng, 1, 1);
+  switch (p.np) {
+    case 0: return launch_pdl(adj_b_kernel<T, 0>, g, b, st, p, gx, gy, nb);
+    case 1: return launch_pdl(adj_b_kernel<T, 1>, g, b, st, p, gx, gy, nb);
+    case 2: return launch_pdl(adj_b_kernel<T, 2>, g, b, st, p, gx, gy, nb);
+    default: return launch_pdl(adj_b_kernel<T, 3>, g, b, st, p, gx, gy, nb);
+  }
 }
 
 template <typename T>
@@ -740,8 +788,6 @@ cudaError_t launch_sum_terms(const double *terms, long long n, double *out, cuda
 
 template cudaError_t launch_adj_e<float>(const AdjParams<float> &, cudaStream_t);
 template cudaError_t launch_adj_e<double>(const AdjParams<double> &, cudaStream_t);
-template cudaError_t launch_adj_grad<float>(const AdjParams<float> &, cudaStream_t);
-template cudaError_t launch_adj_grad<double>(const AdjParams<double> &, cudaStream_t);
 template cudaError_t launch_adj_b<float>(const AdjParams<float> &, cudaStream_t);
 template cudaError_t launch_adj_b<double>(const AdjParams<double> &, cudaStream_t);
 template cudaError_t launch_adj_init<float>(const AdjParams<float> &, cudaStream_t);

@@ -50,7 +50,6 @@ void tma_boxes(int esz, int e_box[7][2], int b_box[6][2]);
 #define MPB_ADJ_B_BPSM 8
 #endif
 template <typename T> cudaError_t launch_adj_e(const AdjParams<T> &, cudaStream_t);
-template <typename T> cudaError_t launch_adj_grad(const AdjParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_adj_b(const AdjParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_adj_init(const AdjParams<T> &, cudaStream_t);
 template <typename T>
@@ -1646,38 +1645,27 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   // The reverse pass runs on a second stream: the adjoint kernels of one chunk
   // overlap the forward run of the next, which only shares the history buffer
   // the chunk reads (events order the two).
-  // The design gradients of each reverse step run on a third stream beside
-  // adj_b (adj_grad reads what adj_e wrote and must finish before the next
-  // adj_e overwrites it).
   struct RevStream {
-    cudaStream_t s = nullptr, g = nullptr;
+    cudaStream_t s = nullptr;
     cudaEvent_t fwd[2] = {nullptr, nullptr}, rev[2] = {nullptr, nullptr};
-    cudaEvent_t e_done = nullptr, g_done = nullptr;
     bool used[2] = {false, false};
     ~RevStream() {
-      for (cudaStream_t q : {s, g})
-        if (q) {
-          cudaStreamSynchronize(q);
-          cudaStreamDestroy(q);
-        }
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
       for (int q = 0; q < 2; ++q) {
         if (fwd[q]) cudaEventDestroy(fwd[q]);
         if (rev[q]) cudaEventDestroy(rev[q]);
       }
-      if (e_done) cudaEventDestroy(e_done);
-      if (g_done) cudaEventDestroy(g_done);
     }
   } rs;
-  if ((e = cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaStreamCreateWithFlags(&rs.g, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking)) != cudaSuccess)
     return cuda_err(c, e, "cudaStreamCreate");
   for (int q = 0; q < 2; ++q)
     if ((e = cudaEventCreateWithFlags(&rs.fwd[q], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&rs.rev[q], cudaEventDisableTiming)) != cudaSuccess)
       return cuda_err(c, e, "cudaEventCreate");
-  if ((e = cudaEventCreateWithFlags(&rs.e_done, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaEventCreateWithFlags(&rs.g_done, cudaEventDisableTiming)) != cudaSuccess)
-    return cuda_err(c, e, "cudaEventCreate");
   int cur = 0;  // history buffer of the chunk being run forward
   AdjParams<T> p = AdjParams<T>();
   for (int q = 0; q < 3; ++q) {
@@ -1887,15 +1875,11 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       p.obx = slot_b(n - n0, 0);
       p.oby = slot_b(n - n0, 1);
       p.add_obj = n >= 1;
+      // adj_e, then adj_b with the step's design gradients, chained by
+      // programmatic dependent launch
       if ((err = launch_adj_e<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint E kernel");
-      if ((err = cudaEventRecord(rs.e_done, rs.s)) != cudaSuccess ||
-          (err = cudaStreamWaitEvent(rs.g, rs.e_done, 0)) != cudaSuccess)
-        return cuda_err(c, err, "event");
-      if ((err = launch_adj_grad<T>(p, rs.g)) != cudaSuccess) return cuda_err(c, err, "adjoint gradient kernel");
-      if ((err = cudaEventRecord(rs.g_done, rs.g)) != cudaSuccess) return cuda_err(c, err, "event");
       if ((err = launch_adj_b<T>(p, rs.s)) != cudaSuccess) return cuda_err(c, err, "adjoint B kernel");
-      if ((err = cudaStreamWaitEvent(rs.s, rs.g_done, 0)) != cudaSuccess) return cuda_err(c, err, "event");
-      c->launches += 3;
+      c->launches += 2;
     }
     if ((err = cudaEventRecord(rs.rev[cur], rs.s)) != cudaSuccess) return cuda_err(c, err, "event");
     rs.used[cur] = true;

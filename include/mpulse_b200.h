@@ -57,7 +57,7 @@
 extern "C" {
 #endif
 
-#define MP_ABI_VERSION 1
+#define MP_ABI_VERSION 2
 #define MP_MAX_POLES 3
 #define MP_MAX_SOURCES 4
 
@@ -203,6 +203,29 @@ typedef struct mp_config {
    * planes and the interior.  A cell with factors 1 and eps_infinity = eps
    * gives the same results as a cell outside the box. */
   int design_box[6];
+
+  /* Plasma plug-ins of the PLRC solvers (src/fdtd_plrc.t:431-436), PLRC
+   * solvers only, global-load staging only, no design box, no adjoint.
+   * "plasma" (PlasmaDensity, src/plasmadensity.cpp:18-61): every step, before
+   * the E half, from I = |E^n|^2: rho <- (rho (1 + n I) + m I^K) / (1 - n I)
+   * with n = dt nu / 2, m = dt mpa, and the conductivity Sigma = mpa Wion
+   * I^(K-1) of the E update (numer - Sigma dt / 2, denom + Sigma dt / 2).
+   * "plasma_current" (PlasmaCurrent, src/plasmacurrent.cpp:42-74): the
+   * current J <- (J (1 - gamma dt / 2) - em dt E^n (rho + rho_bg)) /
+   * (1 + gamma dt / 2), added to the E update after the other currents.
+   * The density and the current are device state, named "PlasmaDensity" and
+   * "PlasmaJx" / "PlasmaJy" / "PlasmaJz" as in MPulse's Storage, kept on the
+   * planes 1..nz the E half updates (MPulse also evolves them on its ghost
+   * cells, where they never reach the fields). */
+  int plasma;               /* 1: the "plasma" plug-in */
+  double plasma_nu;         /* nu: avalanche ionisation (default 1) */
+  double plasma_mpa;        /* mpa: multi-photon ionisation (default 1) */
+  double plasma_wion;       /* Wion: ionisation energy (default 1) */
+  int plasma_k;             /* K: order of the multi-photon term (default 5) */
+  int plasma_current;       /* 1: the "plasma_current" plug-in */
+  double plasma_em;         /* em: e/m of the carriers (default 1) */
+  double plasma_gamma;      /* gamma: friction (default 0.1) */
+  double plasma_rho_bg;     /* rho_bg: constant background density (default 0) */
 } mp_config;
 
 /* Objectives of mp_objective / mp_adjoint (additions to MPulse). */
@@ -247,9 +270,11 @@ void mp_destroy(mp_ctx *ctx);
 int mp_set_stream(mp_ctx *ctx, void *cuda_stream);
 
 /* Number of doubles of the host buffer for field `name`.  Names follow
- * MPulse's Storage: "Ex" "Ey" "Ez" "Bx" "By" "Bz" (fdtd_plrc.cpp:17-23) and the
+ * MPulse's Storage: "Ex" "Ey" "Ez" "Bx" "By" "Bz" (fdtd_plrc.cpp:17-23), the
  * PLRC accumulators "PsiR<n><c>" / "PsiI<n><c>" with n = 1..3, c = x, y, z
- * (fdtd_plrc.cpp:35-57), all in the plane layout described above. */
+ * (fdtd_plrc.cpp:35-57) and, with the plasma plug-ins, "PlasmaDensity" and
+ * "PlasmaJx" / "PlasmaJy" / "PlasmaJz" (plasmadensity.cpp:17,
+ * plasmacurrent.cpp:35-39), all in the plane layout described above. */
 int mp_field_size(mp_ctx *ctx, const char *name, size_t *count);
 
 /* Copies a host field into the device state (converted to the device form). */

@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 
-MP_ABI_VERSION = 1
+MP_ABI_VERSION = 2
 MP_MAX_POLES = 3
 MP_MAX_SOURCES = 4
 MP_NOALLOC_MAX_PLANES = 16384
@@ -49,6 +49,7 @@ MP_OBJ_E2_BOX, MP_OBJ_SZ_PLANE = 1, 2
 FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz")
 DESIGN_NAMES = ("DesignEps", "DesignDepsScale", "DesignChiScale")
 PSI_NAMES = tuple(f"Psi{ri}{n}{c}" for ri in "RI" for n in (1, 2, 3) for c in "xyz")
+PLASMA_NAMES = ("PlasmaDensity", "PlasmaJx", "PlasmaJy", "PlasmaJz")
 
 
 class LorentzPole(C.Structure):
@@ -113,6 +114,15 @@ class Config(C.Structure):
         ("staging", C.c_int),
         ("device", C.c_int),
         ("design_box", C.c_int * 6),
+        ("plasma", C.c_int),
+        ("plasma_nu", C.c_double),
+        ("plasma_mpa", C.c_double),
+        ("plasma_wion", C.c_double),
+        ("plasma_k", C.c_int),
+        ("plasma_current", C.c_int),
+        ("plasma_em", C.c_double),
+        ("plasma_gamma", C.c_double),
+        ("plasma_rho_bg", C.c_double),
     ]
 
     def field_count(self) -> int:
@@ -237,6 +247,13 @@ def default_config() -> Config:
     c.staging = MP_STAGING_AUTO
     c.device = 0
     c.design_box[:] = (1, 0, 1, 0, 1, 0)
+    c.plasma = 0
+    c.plasma_nu = c.plasma_mpa = c.plasma_wion = 1.0
+    c.plasma_k = 5
+    c.plasma_current = 0
+    c.plasma_em = 1.0
+    c.plasma_gamma = 0.1
+    c.plasma_rho_bg = 0.0
     return c
 
 

@@ -122,6 +122,7 @@ struct mp_ctx {
   bool pre_pending[2] = {false, false};  // a side-stream write of buffer b may be in flight
   GaussBeam *gauss = nullptr;  // gauss_inject state when the last injector is one
   double *d_wcoef = nullptr;
+  void *plasma[4] = {nullptr, nullptr, nullptr, nullptr};  // PlasmaDensity, PlasmaJx, PlasmaJy, PlasmaJz
   int *d_status = nullptr;
   int *h_status = nullptr;
   unsigned long long *d_kerr = nullptr;  // Kerr solves and Newton iterations since the last mp_kerr_counts
@@ -271,6 +272,14 @@ int validate(const mp_config *c) {
     if (c->staging == MP_STAGING_TMA)
       return set_err(nullptr, MP_ERR_UNSUPPORTED, "design regions use the global-load kernels (staging GLOBAL/AUTO)");
   }
+  if (c->plasma || c->plasma_current) {
+    if (!plrc) return set_err(nullptr, MP_ERR_INVALID, "the plasma plug-ins belong to the PLRC solvers (fdtd_plrc.t:431-436)");
+    if (c->plasma && (c->plasma_k < 1 || c->plasma_k > 64))
+      return set_err(nullptr, MP_ERR_INVALID, "plasma K %d outside 1..64", c->plasma_k);
+    if (c->staging == MP_STAGING_TMA)
+      return set_err(nullptr, MP_ERR_UNSUPPORTED, "the plasma plug-ins use the global-load kernels (staging GLOBAL/AUTO)");
+    if (db[0] <= db[1]) return set_err(nullptr, MP_ERR_UNSUPPORTED, "the plasma plug-ins and a design region together");
+  }
   if (c->staging == MP_STAGING_TMA && (c->nx % kTmaTileX != 0 || c->ny % kTmaTileY != 0))
     return set_err(nullptr, MP_ERR_UNSUPPORTED, "TMA staging needs nx a multiple of %d and ny of %d", kTmaTileX,
                    kTmaTileY);
@@ -332,6 +341,25 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
       ep.pxi[s][q] = T(coef[1][s][q]);
       ep.pC[s][q] = T(coef[2][s][q]);
     }
+  if (c->plasma[0]) {
+    // PlasmaDensity (plasmadensity.cpp:31-35) and PlasmaCurrent
+    // (plasmacurrent.cpp:57-59) constants
+    ep.rho = static_cast<T *>(c->plasma[0]);
+    for (int a = 0; a < 3; ++a) ep.pj[a] = static_cast<T *>(c->plasma[1 + a]);
+    ep.pl_density = g.plasma ? 1 : 0;
+    ep.pl_current = g.plasma_current ? 1 : 0;
+    ep.pl_km = g.plasma_k - 1;
+    ep.pl_n = T(0.5 * g.dt * g.plasma_nu);
+    ep.pl_m = T(g.dt * g.plasma_mpa);
+    ep.pl_w = T(g.plasma_mpa * g.plasma_wion);
+    ep.pl_gdtn = T(1 - 0.5 * g.plasma_gamma * g.dt);
+    ep.pl_gdtd = T(1 + 0.5 * g.plasma_gamma * g.dt);
+    ep.pl_emdt = T(g.plasma_em * g.dt);
+    ep.pl_rho_bg = T(g.plasma_rho_bg);
+  }
+  ep.denom_t = T(denom);
+  ep.denom_d = denom;
+  ep.chi_raw = g.chi;
   ep.numer = T(numer);
   ep.inv_denom = T(1.0 / denom);
   ep.numer_lo = T(numer - double(ep.numer));
@@ -468,6 +496,8 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   } while (0)
 
   for (int f = 0; f < 6; ++f) MPB_TRY(dalloc(c, &c->F[f], c->fcount * c->esz), "field allocation");
+  if (g.plasma || g.plasma_current)
+    for (int q = 0; q < 4; ++q) MPB_TRY(dalloc(c, &c->plasma[q], c->fcount * c->esz), "plasma allocation");
 
   const bool plrc = c->mode == MODE_PLRC_LIN || c->mode == MODE_PLRC_NONLIN;
   // PLRC: active poles (Delta eps != 0) and their accumulators over the medium
@@ -793,6 +823,15 @@ int resolve(mp_ctx *c, const char *name, FieldView &v) {
       v.nk = c->cfg.nz + 2;
       return MP_OK;
     }
+  static const char *pn[4] = {"PlasmaDensity", "PlasmaJx", "PlasmaJy", "PlasmaJz"};
+  for (int q = 0; q < 4; ++q)
+    if (!strcmp(name, pn[q])) {
+      if (!c->plasma[q]) return set_err(c, MP_ERR_NAME, "%s: no plasma plug-in in this configuration", name);
+      v.base = c->plasma[q];
+      v.k0 = 0;
+      v.nk = c->cfg.nz + 2;
+      return MP_OK;
+    }
   if (!strncmp(name, "Psi", 3) && (name[3] == 'R' || name[3] == 'I') && name[4] >= '1' && name[4] <= '3' &&
       name[5] >= 'x' && name[5] <= 'z' && name[6] == 0) {
     const bool plrc = c->mode == MODE_PLRC_LIN || c->mode == MODE_PLRC_NONLIN;
@@ -1047,6 +1086,13 @@ void mp_config_defaults(mp_config *c) {
   c->newton_tol = 1e-9;       // fdtd_plrc.cpp:414
   c->device = 0;
   c->design_box[0] = c->design_box[2] = c->design_box[4] = 1;  // empty: x0 > x1
+  c->plasma = 0;
+  c->plasma_nu = c->plasma_mpa = c->plasma_wion = 1.0;  // plasmadensity.cpp:55-58
+  c->plasma_k = 5;
+  c->plasma_current = 0;
+  c->plasma_em = 1.0;                                   // plasmacurrent.cpp:10-12
+  c->plasma_gamma = 0.1;
+  c->plasma_rho_bg = 0.0;
 }
 
 int mp_create(const mp_config *cfg, mp_ctx **out) {
@@ -1346,6 +1392,8 @@ struct DevBufs {
 std::vector<std::pair<void *, size_t>> state_regions(const mp_ctx *c) {
   std::vector<std::pair<void *, size_t>> r;
   for (int f = 0; f < 6; ++f) r.emplace_back(c->F[f], c->fcount * c->esz);
+  for (int q = 0; q < 4; ++q)
+    if (c->plasma[q]) r.emplace_back(c->plasma[q], c->fcount * c->esz);
   for (int s = 0; s < c->np; ++s)
     for (int a = 0; a < 3; ++a) r.emplace_back(c->psi[s][a], 2 * c->psi_cells * c->esz);
   for (int f = 0; f < 6; ++f)
@@ -1923,6 +1971,7 @@ int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_ep
   if (rc != MP_OK) return rc;
   if (c->mode != MODE_PLRC_LIN && c->mode != MODE_PLRC_NONLIN)
     return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint needs a PLRC solver");
+  if (c->plasma[0]) return set_err(c, MP_ERR_UNSUPPORTED, "the adjoint of the plasma plug-ins is not built");
   if (c->cfg.boundary != MP_BOUNDARY_XY_PERIODIC)
     return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint needs the xy-periodic boundary");
   if (!c->design) return set_err(c, MP_ERR_INVALID, "mp_adjoint needs a design region (mp_config.design_box)");

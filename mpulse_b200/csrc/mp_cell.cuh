@@ -159,6 +159,41 @@ __device__ __forceinline__ T inv_denom_mul(T x, T idn, T idn_lo) {
   return sizeof(T) == 4 ? fma(x, idn, x * idn_lo) : x * idn;
 }
 
+// The plasma plug-ins at one cell, from E^n (before the E update):
+// PlasmaDensity::stepScheme (plasmadensity.cpp:18-49) gives the new density
+// and the conductivity Sigma = mpa Wion I^(K-1) of this step (Sigma is reset
+// every step, fdtd_plrc.t:129), of which the E update takes sig = Sigma dt / 2
+// (fdtd_plrc.cpp:188, :356); PlasmaCurrent::stepScheme
+// (plasmacurrent.cpp:42-74) gives the new current from E^n and the new
+// density.  Same operations and order as the reference.
+template <typename T>
+struct PlasmaCell {
+  T rho, j[3], sig;
+};
+
+template <typename T>
+__device__ __forceinline__ void plasma_cell(const EParams<T> &p, T ex, T ey, T ez, T rho, T j0, T j1, T j2,
+                                            PlasmaCell<T> &pc) {
+  pc.rho = rho;
+  pc.sig = T(0);
+  if (p.pl_density) {
+    const T I = ex * ex + ey * ey + ez * ez;
+    T IKm = T(1);  // util.h ipow: K - 1 products
+    for (int q = 0; q < p.pl_km; ++q) IKm *= I;
+    const T IK = I * IKm;
+    pc.rho = (rho * (T(1) + p.pl_n * I) + p.pl_m * IK) / (T(1) - p.pl_n * I);
+    pc.sig = T(0.5) * (p.pl_w * IKm) * p.dt;
+  }
+  if (p.pl_current) {
+    const T r = pc.rho + p.pl_rho_bg;
+    pc.j[0] = (j0 * p.pl_gdtn - p.pl_emdt * ex * r) / p.pl_gdtd;
+    pc.j[1] = (j1 * p.pl_gdtn - p.pl_emdt * ey * r) / p.pl_gdtd;
+    pc.j[2] = (j2 * p.pl_gdtn - p.pl_emdt * ez * r) / p.pl_gdtd;
+  } else {
+    pc.j[0] = pc.j[1] = pc.j[2] = T(0);
+  }
+}
+
 // Values one E update reads: B at the cell and its x-1, y-1, z-1 neighbours
 // (the ones the curl uses) and the old E.
 template <typename T>
@@ -236,14 +271,22 @@ __device__ __forceinline__ void cell_coef(const EParams<T> &p, int i, int j, int
 
 // SPECIAL = false: the caller guarantees that no CPML face contains the cell
 // and that k is no injection plane; the face and source code is left out.
-template <typename T, int MODE, int NP, bool DESIGN = false, bool SPECIAL = true>
+// PLASMA: *pc holds the plasma plug-ins' values of the cell (plasma_cell).
+template <typename T, int MODE, int NP, bool DESIGN = false, bool SPECIAL = true, bool PLASMA = false>
 __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k, long long col, bool med,
                                        unsigned cmask, const EIn<T> &v, T ikx, T iky, T ikz,
                                        typename Vec2<T>::type (&q)[NP > 0 ? NP : 1][3], T &exn, T &eyn,
-                                       T &ezn, KerrCount &kc) {
+                                       T &ezn, KerrCount &kc, const PlasmaCell<T> *pc = nullptr) {
   const T dt = p.dt;
   CellCoef<T, NP> lc;
   cell_coef<T, NP, DESIGN>(p, i, j, k, med, lc);
+  if (PLASMA && med && p.pl_density) {
+    // numer - sig and denom + sig (fdtd_plrc.cpp:188-196, :356-359)
+    lc.numer = lc.numer - pc->sig;
+    lc.inv_denom = T(1) / (p.denom_t + pc->sig);
+    lc.inv_denom_lo = T(0);
+    lc.chi_over_denom = p.chi_raw / (p.denom_d + (double)pc->sig);
+  }
   // ---- loads of the CPML psi of the faces containing the cell, and of the
   // injection plane
   T cp0[6], cp1[6], cb[6], cc[6];
@@ -299,6 +342,11 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       jy += sb;
     }
   }
+  if (PLASMA) {  // the plasma current, after the other currents
+    jx += pc->j[0];
+    jy += pc->j[1];
+    jz += pc->j[2];
+  }
 
   // curl_kappa B (fdtd_plrc.cpp:207-244)
   const T cbx = (v.bz - v.bz_ym) * iky - (v.by - v.by_km) * ikz;
@@ -332,9 +380,16 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     }
   } else if (!med) {
     // background: no poles, no Kerr term
-    exn = (p.eps_bg * ex + dt_mul(dt, dtl, cbx + jx)) * p.inv_eps_bg;
-    eyn = (p.eps_bg * ey + dt_mul(dt, dtl, cby + jy)) * p.inv_eps_bg;
-    ezn = (p.eps_bg * ez + dt_mul(dt, dtl, cbz + jz)) * p.inv_eps_bg;
+    if (PLASMA && p.pl_density) {
+      const T nb = p.eps_bg - pc->sig, ib = T(1) / (p.eps_bg + pc->sig);
+      exn = (nb * ex + dt_mul(dt, dtl, cbx + jx)) * ib;
+      eyn = (nb * ey + dt_mul(dt, dtl, cby + jy)) * ib;
+      ezn = (nb * ez + dt_mul(dt, dtl, cbz + jz)) * ib;
+    } else {
+      exn = (p.eps_bg * ex + dt_mul(dt, dtl, cbx + jx)) * p.inv_eps_bg;
+      eyn = (p.eps_bg * ey + dt_mul(dt, dtl, cby + jy)) * p.inv_eps_bg;
+      ezn = (p.eps_bg * ez + dt_mul(dt, dtl, cbz + jz)) * p.inv_eps_bg;
+    }
   } else {
     T Px = T(0), Py = T(0), Pz = T(0);
     if (NP > 0) {

@@ -121,6 +121,17 @@ struct EParams {
   unsigned long long *kerr_count;  // [0] Kerr solves, [1] their Newton iterations (accumulated)
   long long n_field;      // elements of each field and history array
   long long n_psi;        // pairs of each PLRC accumulator array
+
+  // Plasma plug-ins: PlasmaDensity (plasmadensity.cpp:18-49) and PlasmaCurrent
+  // (plasmacurrent.cpp:42-74), state in the field layout (planes 1..nz used);
+  // rho == nullptr: no plasma
+  T *rho, *pj[3];
+  int pl_density, pl_current;
+  int pl_km;                        // K - 1
+  T pl_n, pl_m, pl_w;               // dt nu / 2, dt mpa, mpa Wion
+  T pl_gdtn, pl_gdtd, pl_emdt, pl_rho_bg;  // 1 - gamma dt / 2, 1 + gamma dt / 2, em dt, rho_bg
+  T denom_t;                        // the medium's denominator without the conductivity
+  double denom_d, chi_raw;          // the same in FP64, and chi
 };
 
 template <typename T>

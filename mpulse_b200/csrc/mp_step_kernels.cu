@@ -82,7 +82,7 @@
 
 namespace mpb {
 
-template <typename T, int MODE, int NP, bool DESIGN>
+template <typename T, int MODE, int NP, bool DESIGN, bool PLASMA = false>
 __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y,
                                   (sizeof(T) == 4 ? MPB_E_MIN_THREADS_F : MPB_E_MIN_THREADS) / (32 * MPB_E_BLOCK_Y))
     e_half_kernel(const EParams<T> p) {
@@ -148,15 +148,36 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y,
 #pragma unroll
         for (int c = 0; c < 3; ++c) q[n][c] = ld_c(reinterpret_cast<const T2 *>(p.psi[n][c]), pi, p.n_psi, st);
     }
+    PlasmaCell<T> pc;
+    if (PLASMA) {
+      const T r0 = ld_c(p.rho, base + col, nf, st);
+      T j0 = T(0), j1 = T(0), j2 = T(0);
+      if (p.pl_current) {
+        j0 = ld_c(p.pj[0], base + col, nf, st);
+        j1 = ld_c(p.pj[1], base + col, nf, st);
+        j2 = ld_c(p.pj[2], base + col, nf, st);
+      }
+      plasma_cell(p, v.ex, v.ey, v.ez, r0, j0, j1, j2, pc);
+    }
     T exn, eyn, ezn;
     if (warp_xy || z_face_plane(p.cpml, k) || (k >= srck.x && k <= srck.y))
-      e_cell<T, MODE, NP, DESIGN, true>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
+      e_cell<T, MODE, NP, DESIGN, true, PLASMA>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc,
+                                                &pc);
     else
-      e_cell<T, MODE, NP, DESIGN, false>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn, kc);
+      e_cell<T, MODE, NP, DESIGN, false, PLASMA>(p, i, j, k, col, med, cmask, v, ikx, iky, ikz, q, exn, eyn, ezn,
+                                                 kc, &pc);
     // ---- stores
     st_c(Ex, base + col, nf, st, exn);
     st_c(Ey, base + col, nf, st, eyn);
     st_c(Ez, base + col, nf, st, ezn);
+    if (PLASMA) {
+      st_c(p.rho, base + col, nf, st, pc.rho);
+      if (p.pl_current) {
+        st_c(p.pj[0], base + col, nf, st, pc.j[0]);
+        st_c(p.pj[1], base + col, nf, st, pc.j[1]);
+        st_c(p.pj[2], base + col, nf, st, pc.j[2]);
+      }
+    }
     if (DESIGN && p.hist[0]) {
       st_c(p.hist[0], base + col, nf, st, exn);
       st_c(p.hist[1], base + col, nf, st, eyn);
@@ -461,32 +482,37 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
 // Launchers (called from mp_api.cu)
 
 
-template <typename T, int MODE, bool DESIGN>
+template <typename T, int MODE, bool DESIGN, bool PLASMA = false>
 static cudaError_t launch_e_np(const EParams<T> &p, int np, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
   const dim3 g((p.nx + 31) / 32, (p.ny + MPB_E_BLOCK_Y - 1) / MPB_E_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk),
       b(32, MPB_E_BLOCK_Y, 1);
   switch (np) {
-    case 0: e_half_kernel<T, MODE, 0, DESIGN><<<g, b, 0, st>>>(p); break;
-    case 1: e_half_kernel<T, MODE, 1, DESIGN><<<g, b, 0, st>>>(p); break;
-    case 2: e_half_kernel<T, MODE, 2, DESIGN><<<g, b, 0, st>>>(p); break;
-    default: e_half_kernel<T, MODE, 3, DESIGN><<<g, b, 0, st>>>(p); break;
+    case 0: e_half_kernel<T, MODE, 0, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
+    case 1: e_half_kernel<T, MODE, 1, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
+    case 2: e_half_kernel<T, MODE, 2, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
+    default: e_half_kernel<T, MODE, 3, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
   }
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_e_half(const EParams<T> &p, int mode, int np, cudaStream_t st) {
-  // design regions exist only with the PLRC solvers
+  // design regions and the plasma plug-ins exist only with the PLRC solvers
+  // (and not together)
   const bool design = p.design.x0 <= p.design.x1;
+  const bool plasma = p.rho != nullptr;
   switch (mode) {
     case MODE_PLAIN: return launch_e_np<T, MODE_PLAIN, false>(p, 0, st);
     case MODE_NL: return launch_e_np<T, MODE_NL, false>(p, 0, st);
     case MODE_PLRC_LIN:
-      return design ? launch_e_np<T, MODE_PLRC_LIN, true>(p, np, st) : launch_e_np<T, MODE_PLRC_LIN, false>(p, np, st);
+      return design   ? launch_e_np<T, MODE_PLRC_LIN, true>(p, np, st)
+             : plasma ? launch_e_np<T, MODE_PLRC_LIN, false, true>(p, np, st)
+                      : launch_e_np<T, MODE_PLRC_LIN, false>(p, np, st);
     default:
-      return design ? launch_e_np<T, MODE_PLRC_NONLIN, true>(p, np, st)
-                    : launch_e_np<T, MODE_PLRC_NONLIN, false>(p, np, st);
+      return design   ? launch_e_np<T, MODE_PLRC_NONLIN, true>(p, np, st)
+             : plasma ? launch_e_np<T, MODE_PLRC_NONLIN, false, true>(p, np, st)
+                      : launch_e_np<T, MODE_PLRC_NONLIN, false>(p, np, st);
   }
 }
 

@@ -30,6 +30,21 @@ ParameterMap *GpuCpmlBlock::MakeParamMap(ParameterMap *pm) {
   return pm;
 }
 
+ParameterMap *GpuPlasmaBlock::MakeParamMap(ParameterMap *pm) {
+  pm = CurrentFactory::MakeParamMap(pm);
+  if (current) {
+    (*pm)["em"] = WParameter(new ParameterValue<double>(&em, 1.0));
+    (*pm)["gamma"] = WParameter(new ParameterValue<double>(&gamma, 0.1));
+    (*pm)["rho_bg"] = WParameter(new ParameterValue<double>(&rho_bg, 0.0));
+  } else {
+    (*pm)["nu"] = WParameter(new ParameterValue<double>(&nu, 1.0));
+    (*pm)["mpa"] = WParameter(new ParameterValue<double>(&mpa, 1.0));
+    (*pm)["Wion"] = WParameter(new ParameterValue<double>(&Wion, 1.0));
+    (*pm)["K"] = WParameter(new ParameterValue<int>(&K, 5));
+  }
+  return pm;
+}
+
 ParameterMap *GpuSourceBlock::MakeParamMap(ParameterMap *pm) {
   pm = CurrentFactory::MakeParamMap(pm);
   (*pm)["d"] = WParameter(new ParameterValue<int>(&distance, 15));
@@ -118,6 +133,7 @@ void GpuSourceBlock::fill(mp_source &s) const {
 FDTD_GPU::FDTD_GPU(int solver_)
     : solver(solver_), storage(0), ctx(0), hostDirty(true), stepsSinceSync(0) {
   for (int f = 0; f < 6; ++f) pF[f] = 0;
+  for (int q = 0; q < 4; ++q) pPlasma[q] = 0;
 }
 
 FDTD_GPU::~FDTD_GPU() { mp_destroy(ctx); }
@@ -154,6 +170,8 @@ ParameterMap *FDTD_GPU::MakeParamMap(ParameterMap *pm) {
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_GAUSS_BEAM>, CurrentFactory>(&blocks));
   (*pm)["focused_pulse_inject"] =
       WParameter(new ParameterRebuild<GpuSourceBlockT<MP_SOURCE_FOCUSED_PULSE>, CurrentFactory>(&blocks));
+  (*pm)["plasma"] = WParameter(new ParameterRebuild<GpuPlasmaBlockT<0>, CurrentFactory>(&blocks));
+  (*pm)["plasma_current"] = WParameter(new ParameterRebuild<GpuPlasmaBlockT<1>, CurrentFactory>(&blocks));
   return pm;
 }
 
@@ -210,9 +228,26 @@ void FDTD_GPU::initStorage(Storage *storage_) {
         exit(-1);
       }
       sb->fill(cfg.sources[cfg.n_sources++]);
+    } else if (GpuPlasmaBlock *pb = dynamic_cast<GpuPlasmaBlock *>(*it)) {
+      if (pb->current) {
+        cfg.plasma_current = 1;
+        cfg.plasma_em = pb->em;
+        cfg.plasma_gamma = pb->gamma;
+        cfg.plasma_rho_bg = pb->rho_bg;
+      } else {
+        cfg.plasma = 1;
+        cfg.plasma_nu = pb->nu;
+        cfg.plasma_mpa = pb->mpa;
+        cfg.plasma_wion = pb->Wion;
+        cfg.plasma_k = pb->K;
+      }
     }
   }
   check(mp_create(&cfg, &ctx), "mp_create");
+  // the plasma plug-ins' grids (plasmadensity.cpp:17, plasmacurrent.cpp:35-39)
+  const char *plasmaNames[4] = {"PlasmaDensity", "PlasmaJx", "PlasmaJy", "PlasmaJz"};
+  for (int q = 0; q < 4; ++q)
+    pPlasma[q] = (cfg.plasma || cfg.plasma_current) ? storage->addGrid(plasmaNames[q]) : 0;
   // the grids the rest of MPulse sees (FDTD_PLRCCore::coreInitStorage,
   // fdtd_plrc.cpp:17-23, :59-65)
   for (int f = 0; f < 6; ++f) pF[f] = storage->addGrid(kFieldNames[f]);
@@ -241,9 +276,12 @@ void FDTD_GPU::upload() {
 void FDTD_GPU::download() {
   const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
   std::vector<double> h(size_t(nz + 2) * ny * nx);
-  for (int f = 0; f < 6; ++f) {
-    check(mp_download(ctx, kFieldNames[f], &h[0], h.size()), "mp_download");
-    DataGrid &G = *pF[f];
+  const char *plasmaNames[4] = {"PlasmaDensity", "PlasmaJx", "PlasmaJy", "PlasmaJz"};
+  for (int f = 0; f < 10; ++f) {
+    DataGrid *pG = f < 6 ? pF[f] : pPlasma[f - 6];
+    if (!pG) continue;
+    check(mp_download(ctx, f < 6 ? kFieldNames[f] : plasmaNames[f - 6], &h[0], h.size()), "mp_download");
+    DataGrid &G = *pG;
     for (int k = 0; k <= nz + 1; ++k)
       for (int j = 0; j <= ny + 1; ++j)
         for (int i = 0; i <= nx + 1; ++i) {

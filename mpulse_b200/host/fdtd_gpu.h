@@ -6,8 +6,9 @@
 // the same defaults as FDTD_PLRCSolver (src/fdtd_plrc.t:411-473,
 // src/fdtd_plrc.cpp:461-465), FDTD_Plain (src/fdtd_plain.cpp) and
 // FDTD_Nonlinear (src/fdtd_nl.cpp:146-153), including the nested plug-in blocks
-// cpml_border, cpml_border_1d, wave_inject, plane_gauss_inject and
-// short_pulse_inject.  Those blocks do not create host Currents here: their
+// cpml_border, cpml_border_1d, wave_inject, plane_gauss_inject,
+// short_pulse_inject, gauss_inject, focused_pulse_inject, plasma and
+// plasma_current.  Those blocks do not create host Currents here: their
 // parameters configure the device context, which computes the CPML psi fields
 // and the TF/SF planes inside the step kernels.
 //
@@ -78,6 +79,30 @@ class GpuSourceBlockT : public GpuSourceBlock {
   GpuSourceBlockT() : GpuSourceBlock(KIND) {}
 };
 
+// Parameters of the plasma plug-ins of FDTD_PLRCSolver (fdtd_plrc.t:431-436):
+// "plasma" (PlasmaDensity::MakeParamMap, plasmadensity.cpp:52-61) and
+// "plasma_current" (PlasmaCurrentFactory::MakeParamMap,
+// plasmacurrent.cpp:6-15).  The device context computes both inside the E
+// half-step kernel.
+class GpuPlasmaBlock : public CurrentFactory {
+ public:
+  explicit GpuPlasmaBlock(int current_) : current(current_) {}
+  void initCurrents(Storage *, FieldSolver *) {}
+  int current;  // 0: plasma (density), 1: plasma_current
+  double nu, mpa, Wion;
+  int K;
+  double em, gamma, rho_bg;
+
+ protected:
+  ParameterMap *MakeParamMap(ParameterMap *pm = NULL);
+};
+
+template <int CURRENT>
+class GpuPlasmaBlockT : public GpuPlasmaBlock {
+ public:
+  GpuPlasmaBlockT() : GpuPlasmaBlock(CURRENT) {}
+};
+
 class FDTD_GPU : public FieldSolver {
  public:
   explicit FDTD_GPU(int solver_);
@@ -113,6 +138,7 @@ class FDTD_GPU : public FieldSolver {
   std::list<CurrentFactory *> blocks;
 
   DataGrid *pF[6];
+  DataGrid *pPlasma[4];  // PlasmaDensity, PlasmaJx..z (when the plug-ins are on)
 };
 
 template <int SOLVER>

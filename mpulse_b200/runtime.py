@@ -243,6 +243,10 @@ class Simulation:
         """J and its gradient with respect to the design maps (mp_adjoint):
         {"DesignEps": .., "DesignDepsScale": .., "DesignChiScale": ..}."""
         shape = abi.design_shape(self.cfg)
+        if shape is None:  # no design box: the library rejects the call
+            J = C.c_double()
+            self._check(lib().mp_adjoint(self._h, C.byref(adj), C.byref(J), None, None, None))
+            return J.value, {}
         n = int(np.prod(shape))
         g = [np.empty(n) for _ in range(3)]
         J = C.c_double()

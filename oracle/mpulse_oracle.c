@@ -102,6 +102,9 @@ typedef struct mpo_sim {
   int design;
   box3 dbox;
   double *deps, *dscale, *dchi;
+  /* plasma plug-ins (fdtd_plrc.t:431-436): density, conductivity Sigma
+   * (reset every step, fdtd_plrc.t:129), plasma current; full ghost grids */
+  double *rho, *Sig, *PJ[3];
   long long time;
   int newton_fail;
   char err[256];
@@ -885,7 +888,7 @@ static void inc_add(mpo_sim *s, inc_layer *L, int writer, double **tot) {
       }
 }
 
-static int has_currents(const mpo_sim *s) { return s->nE + s->nIE > 0; }
+static int has_currents(const mpo_sim *s) { return s->nE + s->nIE > 0 || s->cfg.plasma_current; }
 static int has_mag_currents(const mpo_sim *s) { return s->nH + s->nIH > 0; }
 
 static void sum_currents(mpo_sim *s, int mag) {
@@ -912,6 +915,57 @@ static void sum_currents(mpo_sim *s, int mag) {
     }
     inc_add(s, L, writer, tot);
   }
+  /* the plasma current last, over its full grid (plasma_current listed after
+   * the CPML and injector blocks) */
+  if (!mag && s->cfg.plasma_current)
+    for (int c = 0; c < 3; ++c)
+      for (size_t g = 0; g < n; ++g) tot[c][g] += s->PJ[c][g];
+}
+
+/* util.h ipow: r = 1, then K times r *= x. */
+static double plasma_ipow(double x, int e) {
+  double r = 1.0;
+  for (int q = 0; q < e; ++q) r *= x;
+  return r;
+}
+
+/* PlasmaDensity::stepScheme (plasmadensity.cpp:18-49): over every stored cell
+ * (ghosts included), from E^n. */
+static void plasma_density_step(mpo_sim *s) {
+  const mp_config *c = &s->cfg;
+  const double dt = c->dt;
+  const double nn = 0.5 * dt * c->plasma_nu;
+  const double m = dt * c->plasma_mpa;
+  const double w = c->plasma_mpa * c->plasma_wion;
+  const int Km = c->plasma_k - 1;
+  const size_t n = (size_t)s->NX * s->NY * s->NZ;
+  for (size_t g = 0; g < n; ++g) {
+    const double ex = s->F[0][g], ey = s->F[1][g], ez = s->F[2][g];
+    const double In = ex * ex + ey * ey + ez * ez;  /* I of the reference (I is complex.h's unit) */
+    const double IKm = plasma_ipow(In, Km);
+    const double IK = In * IKm;
+    s->rho[g] = (s->rho[g] * (1 + nn * In) + m * IK) / (1 - nn * In);
+    s->Sig[g] += w * IKm;
+  }
+}
+
+/* PlasmaCurrent::stepScheme (plasmacurrent.cpp:42-74): cells low..high-1 of
+ * every axis, from E^n and the density of this step. */
+static void plasma_current_step(mpo_sim *s) {
+  const mp_config *c = &s->cfg;
+  const double dt = c->dt;
+  const double gdtn = 1 - 0.5 * c->plasma_gamma * dt;
+  const double gdtd = 1 + 0.5 * c->plasma_gamma * dt;
+  const double emdt = c->plasma_em * dt;
+  for (int i = 0; i < s->NX - 1; ++i)
+    for (int j = 0; j < s->NY - 1; ++j)
+      for (int k = 0; k < s->NZ - 1; ++k) {
+        const size_t g = IDX(s, i, j, k);
+        const double rho = s->rho[g] + c->plasma_rho_bg;
+        s->PJ[0][g] = (s->PJ[0][g] * gdtn - emdt * s->F[0][g] * rho) / gdtd;
+        s->PJ[1][g] = (s->PJ[1][g] * gdtn - emdt * s->F[1][g] * rho) / gdtd;
+        s->PJ[2][g] = (s->PJ[2][g] * gdtn - emdt * s->F[2][g] * rho) / gdtd;
+      }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -969,7 +1023,8 @@ static void plrc_step_d(mpo_sim *s, int i, int j, int k, double Jx, double Jy, d
   }
   const double eps = med ? eps_c : c->eps_bg;
   const double sumChi0 = med ? sc * s->sumChi0 : 0.0, sumXi0 = med ? sc * s->sumXi0 : 0.0;
-  const double sigma = 0.5 * 0.0 * dt; /* Sigma = 0 each step (fdtd_plrc.t:129) */
+  /* Sigma: zero each step (fdtd_plrc.t:129) plus the plasma density's term */
+  const double sigma = 0.5 * (s->Sig ? s->Sig[g] : 0.0) * dt;
   const double cbx = (Bz[g] - Bz[IDX(s, i, j - 1, k)]) / kappaEdy - (By[g] - By[IDX(s, i, j, k - 1)]) / kappaEdz;
   const double cby = (Bx[g] - Bx[IDX(s, i, j, k - 1)]) / kappaEdz - (Bz[g] - Bz[IDX(s, i - 1, j, k)]) / kappaEdx;
   const double cbz = (By[g] - By[IDX(s, i - 1, j, k)]) / kappaEdx - (Bx[g] - Bx[IDX(s, i, j - 1, k)]) / kappaEdy;
@@ -1057,7 +1112,11 @@ static void plrc_step_b_all(mpo_sim *s) {
 
 /* FDTD_PLRCSolver::stepScheme (fdtd_plrc.t:127-168). */
 static void plrc_step(mpo_sim *s) {
+  const size_t n = (size_t)s->NX * s->NY * s->NZ;
+  if (s->Sig) memset(s->Sig, 0, n * sizeof(double));
+  if (s->cfg.plasma) plasma_density_step(s);
   for (int l = 0; l < s->nE; ++l) cpml_e_step(s, &s->Elay[l]);
+  if (s->cfg.plasma_current) plasma_current_step(s);
   plrc_step_d_all(s);
   for (int l = 0; l < s->nH; ++l) cpml_h_step(s, &s->Hlay[l]);
   plrc_step_b_all(s);
@@ -1218,6 +1277,15 @@ int mpo_create(const mp_config *cfg, mpo_sim **out) {
     }
     add_inc_layers(s, q);
   }
+  if (cfg->plasma || cfg->plasma_current) {
+    if (!plrc) {
+      mpo_destroy(s);
+      return fail(g_create_err, "the plasma plug-ins belong to the PLRC solvers");
+    }
+    s->rho = calloc(n, sizeof(double));
+    s->Sig = calloc(n, sizeof(double));
+    for (int c = 0; c < 3; ++c) s->PJ[c] = calloc(n, sizeof(double));
+  }
   if (has_currents(s))
     for (int c = 0; c < 3; ++c) s->Jt[c] = calloc(n, sizeof(double));
   if (has_mag_currents(s))
@@ -1267,6 +1335,9 @@ void mpo_destroy(mpo_sim *s) {
   free(s->deps);
   free(s->dscale);
   free(s->dchi);
+  free(s->rho);
+  free(s->Sig);
+  for (int c = 0; c < 3; ++c) free(s->PJ[c]);
   free(s);
 }
 
@@ -1280,6 +1351,12 @@ static double *field_by_name(mpo_sim *s, const char *name) {
       name[4] >= '1' && name[4] <= '3' && name[5] >= 'x' && name[5] <= 'z' && name[6] == 0) {
     const int p = name[4] - '1', c = name[5] - 'x';
     return name[3] == 'R' ? s->psiR[p][c] : s->psiI[p][c];
+  }
+  if (s->rho) {
+    if (!strcmp(name, "PlasmaDensity")) return s->rho;
+    if (!strcmp(name, "PlasmaJx")) return s->PJ[0];
+    if (!strcmp(name, "PlasmaJy")) return s->PJ[1];
+    if (!strcmp(name, "PlasmaJz")) return s->PJ[2];
   }
   return NULL;
 }

@@ -81,6 +81,7 @@ class OracleSim:
 
     def __init__(self, cfg: abi.Config):
         self.cfg = cfg
+        self.h = None
         h = C.c_void_p()
         rc = lib().mpo_create(C.byref(cfg), C.byref(h))
         if rc != abi.MP_OK:
@@ -273,6 +274,14 @@ def setup_text(cfg: abi.Config, steps: int, init_file: str | None = None, solver
                     f"toff {s.t_off}"]) + " }")
             else:
                 raise ValueError(f"source kind {s.kind} has no runnable reference plug-in")
+        # the plasma plug-ins (fdtd_plrc.t:431-436): the density is an E-side
+        # optional field, the current is listed after the other currents
+        if cfg.plasma:
+            body.append(f"plasma {{ nu {_fmt(cfg.plasma_nu)} mpa {_fmt(cfg.plasma_mpa)} "
+                        f"Wion {_fmt(cfg.plasma_wion)} K {cfg.plasma_k} }}")
+        if cfg.plasma_current:
+            body.append(f"plasma_current {{ em {_fmt(cfg.plasma_em)} gamma {_fmt(cfg.plasma_gamma)} "
+                        f"rho_bg {_fmt(cfg.plasma_rho_bg)} }}")
     if extra:
         body.append(extra)
     init = f"raw_init {{ file {init_file} }}\n" if init_file else ""

@@ -56,6 +56,14 @@ def make_case(name: str, precision: int = abi.MP_FP64) -> abi.Config:
         s.amp = 1.0
         for key, val in spec.get("src", {}).items():
             setattr(s, key, val)
+    # the plasma plug-ins: "plasma" = (nu, mpa, Wion, K), "plasma_current" =
+    # (em, gamma, rho_bg)
+    if "plasma" in spec:
+        c.plasma = 1
+        c.plasma_nu, c.plasma_mpa, c.plasma_wion, c.plasma_k = spec["plasma"]
+    if "plasma_current" in spec:
+        c.plasma_current = 1
+        c.plasma_em, c.plasma_gamma, c.plasma_rho_bg = spec["plasma_current"]
     return c
 
 
@@ -110,6 +118,19 @@ CASES = {
     "tma_plain_xy": dict(solver=P.MP_SOLVER_PLAIN, n=(32, 24, 12)),
     "tma_nl_xy": dict(solver=P.MP_SOLVER_NL, n=(64, 16, 10), chi=0.3, eps=1.5),
     "tma_lin_vacuum_cpmlz": dict(solver=P.MP_SOLVER_PLRC_LIN, n=(32, 8, 16), poles=(), cpml=P.MP_CPML_Z),
+    # the plasma plug-ins: density (its conductivity in the E update) and
+    # current, together with CPML, an injector, the medium split and Kerr;
+    # the density alone; the current alone on a background density
+    "plasma_nonlin_all_short": dict(solver=P.MP_SOLVER_PLRC_NONLIN, cpml=P.MP_CPML_ALL, cpml_d=4, chi=0.2,
+                                    medium=(10, 24), eps_bg=1.2, sources=(P.MP_SOURCE_SHORT_PULSE,),
+                                    plasma=(0.4, 3.0, 0.7, 2), plasma_current=(0.8, 0.3, 0.05)),
+    "plasma_density_lin_periodic": dict(solver=P.MP_SOLVER_PLRC_LIN, boundary=P.MP_BOUNDARY_PERIODIC,
+                                        plasma=(0.3, 5.0, 1.5, 3)),
+    "plasma_current_lin_cpmlz": dict(solver=P.MP_SOLVER_PLRC_LIN, cpml=P.MP_CPML_Z, medium=(8, 40),
+                                     sources=(P.MP_SOURCE_PLANE_GAUSS,), plasma_current=(1.3, 0.2, 0.4)),
+    "vec_plasma_nonlin_all": dict(solver=P.MP_SOLVER_PLRC_NONLIN, n=(64, 6, 10), cpml=P.MP_CPML_ALL, cpml_d=2,
+                                  chi=0.2, sources=(P.MP_SOURCE_PLANE_WAVE,), src_d=4,
+                                  plasma=(0.4, 2.0, 0.9, 2), plasma_current=(0.9, 0.2, 0.1)),
 }
 
 

@@ -54,15 +54,21 @@ def case_seed(name: str) -> int:
     return sum(map(ord, name)) % 997
 
 
+def case_names(cfg: abi.Config) -> tuple:
+    """The grids a fixture keeps: the fields, and the plasma plug-ins' state."""
+    return abi.FIELD_NAMES + (abi.PLASMA_NAMES if (cfg.plasma or cfg.plasma_current) else ())
+
+
 def write_case(name: str):
     cfg = small_case(name)
     seed = case_seed(name)
     init = random_fields(cfg, seed=seed)
-    out, timing = pyoracle.run_reference(cfg, GOLDEN_STEPS, init)
+    names = case_names(cfg)
+    out, timing = pyoracle.run_reference(cfg, GOLDEN_STEPS, init, names=names)
     np.savez_compressed(
         os.path.join(HERE, f"case_{name}.npz"),
         config=json.dumps(abi.config_to_dict(cfg)), seed=seed, steps=GOLDEN_STEPS,
-        init_sha256=init_digest(init), **{n: out[n] for n in abi.FIELD_NAMES})
+        init_sha256=init_digest(init), **{n: out[n] for n in names})
     print(name, timing["seconds"])
 
 
@@ -82,8 +88,12 @@ def workload_fixture(name: str, cfg: abi.Config, steps: int, init: dict | None, 
 
 
 def main():
+    only = sys.argv[1:]  # case names to (re)write; default: all cases and workloads
     for name in sorted(CASES):
-        write_case(name)
+        if not only or name in only:
+            write_case(name)
+    if only:
+        return
     # the vacuum pulse workload at full size (64^3, 400 steps)
     c1 = configs.c1_vacuum_pulse(abi.MP_FP64)
     workload_fixture("c1_vacuum_pulse_64", c1, 400, configs.c1_initial_fields(c1))

@@ -23,8 +23,12 @@ def workload_files():
 
 
 def load(path):
+    """A fixture and its mp_config.  Fixtures written before a field was added
+    to mp_config lack it and get its default; the ABI version is the
+    library's."""
     d = np.load(path)
     cfg = abi.config_from_dict(json.loads(str(d["config"])))
+    cfg.abi_version = abi.MP_ABI_VERSION
     return d, cfg
 
 

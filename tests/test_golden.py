@@ -23,7 +23,8 @@ def test_oracle_reproduces_reference_case(path):
     for n, v in init.items():
         o.upload(n, v)
     assert o.step(int(d["steps"])) == abi.MP_OK
-    for n in abi.FIELD_NAMES:
+    # the fields, and the plasma plug-ins' density and current where the case has them
+    for n in [n for n in abi.FIELD_NAMES + abi.PLASMA_NAMES if n in d]:
         got = o.download(n)
         if cfg.n_sources and cfg.sources[0].kind in (abi.MP_SOURCE_SHORT_PULSE, abi.MP_SOURCE_GAUSS_BEAM):
             assert rel_l2(got, d[n]) <= 1e-13, n

@@ -24,15 +24,19 @@ GPU_NAMES = {
 
 
 @pytest.mark.parametrize("case", ["nonlin_all_short", "lin_split_cpmlz_gauss", "plain_xy", "nl_periodic",
-                                  "nonlin_three_poles", "nonlin_all_gauss_beam_blocks"])
+                                  "nonlin_three_poles", "nonlin_all_gauss_beam_blocks", "plasma_nonlin_all_short"])
 def test_mpulse_driver_with_gpu_solver(case):
     cfg = make_case(case, abi.MP_FP64)
     init = random_fields(cfg, seed=21)
-    cpu, _ = pyoracle.run_reference(cfg, 20, init)
-    gpu, _ = pyoracle.run_reference(cfg, 20, init, binary=pyoracle.REF_BIN_GPU, solver_name=GPU_NAMES[cfg.solver],
-                                    extra="sync_interval 1")
+    plasma = abi.PLASMA_NAMES if (cfg.plasma or cfg.plasma_current) else ()
+    names = abi.FIELD_NAMES + plasma
+    cpu, _ = pyoracle.run_reference(cfg, 20, init, names=names)
+    gpu, _ = pyoracle.run_reference(cfg, 20, init, names=names, binary=pyoracle.REF_BIN_GPU,
+                                    solver_name=GPU_NAMES[cfg.solver], extra="sync_interval 1")
     for n in abi.FIELD_NAMES:
         assert rel_l2(gpu[n], cpu[n]) <= 1e-12, (n, rel_l2(gpu[n], cpu[n]))
+    for n in plasma:  # the plug-in keeps the plasma state on the planes the E half updates
+        assert rel_l2(gpu[n][1:-1], cpu[n][1:-1]) <= 1e-12, (n, rel_l2(gpu[n][1:-1], cpu[n][1:-1]))
 
 
 def test_sync_interval_keeps_device_state():

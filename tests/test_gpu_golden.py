@@ -23,6 +23,9 @@ def test_gpu_fp64_reproduces_reference_case(path):
         g.step(int(d["steps"]))
         for n in abi.FIELD_NAMES:
             assert rel_l2(g.download(n), d[n]) <= 1e-12, n
+        # the plasma plug-ins' state, on the planes the E half updates
+        for n in [n for n in abi.PLASMA_NAMES if n in d]:
+            assert rel_l2(g.download(n)[1:-1], d[n][1:-1]) <= 1e-12, n
 
 
 @pytest.mark.parametrize("precision,tol", [(abi.MP_FP64, 1e-12), (abi.MP_FP32, 1e-4)])

@@ -42,14 +42,24 @@ def psi_names(cfg):
     return tuple(f"Psi{ri}{n + 1}{c}" for ri in "RI" for n in range(3) if cfg.poles[n].eps != 0 for c in "xyz")
 
 
+def plasma_names(cfg):
+    """The plasma plug-ins' state; the device keeps it on the planes 1..nz the
+    E half updates, so it is compared there."""
+    return abi.PLASMA_NAMES if (cfg.plasma or cfg.plasma_current) else ()
+
+
+def interior(name, a):
+    return a[1:-1] if name in abi.PLASMA_NAMES else a
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_fp64_matches_oracle(case):
     cfg = make_case(case, abi.MP_FP64)
     init = random_fields(cfg, seed=zlib.crc32(case.encode()) % 1000)
-    names = abi.FIELD_NAMES + psi_names(cfg)
+    names = abi.FIELD_NAMES + psi_names(cfg) + plasma_names(cfg)
     got, want = run_pair(cfg, init, STEPS, names)
     for n in names:
-        err = rel_l2(got[n], want[n])
+        err = rel_l2(interior(n, got[n]), interior(n, want[n]))
         assert err <= TOL_FP64, f"{case} {n}: rel-L2 {err:.3e}"
 
 
@@ -66,8 +76,8 @@ def test_fp32_matches_oracle(case):
         for n, v in init.items():
             g.upload(n, v)
         g.step(STEPS)
-        for n in abi.FIELD_NAMES:
-            err = rel_l2(g.download(n), o.download(n))
+        for n in abi.FIELD_NAMES + plasma_names(cfg64):
+            err = rel_l2(interior(n, g.download(n)), interior(n, o.download(n)))
             assert err <= TOL_FP32, f"{case} {n}: rel-L2 {err:.3e}"
 
 
@@ -283,3 +293,28 @@ def test_kerr_counts(case):
     assert want <= iters <= want * cfg.newton_max_iter
     if want:
         assert iters > solves  # the solve from |E^n| takes more than one iteration where E changes
+
+
+def test_plasma_configurations_are_checked():
+    """The plasma plug-ins belong to the PLRC solvers and run on the
+    global-load kernels; the adjoint of them is not built."""
+    cfg = make_case("plasma_nonlin_all_short", abi.MP_FP64)
+    cfg.staging = abi.MP_STAGING_TMA
+    with pytest.raises(runtime.MPulseError) as e:
+        runtime.Simulation(cfg)
+    assert e.value.code == abi.MP_ERR_UNSUPPORTED
+    bad = make_case("plain_xy", abi.MP_FP64)
+    bad.plasma = 1
+    with pytest.raises(runtime.MPulseError) as e:
+        runtime.Simulation(bad)
+    assert e.value.code == abi.MP_ERR_INVALID
+    cfg = make_case("plasma_nonlin_all_short", abi.MP_FP64)
+    with runtime.Simulation(cfg) as g:
+        with pytest.raises(runtime.MPulseError) as e:
+            g.adjoint(abi.adjoint_config(abi.MP_OBJ_E2_BOX, (2, 4, 2, 4, 3, 5), 3))
+        assert e.value.code == abi.MP_ERR_UNSUPPORTED
+    plain = make_case("nonlin_all_short", abi.MP_FP64)
+    with runtime.Simulation(plain) as g:
+        with pytest.raises(runtime.MPulseError) as e:
+            g.download("PlasmaDensity")
+        assert e.value.code == abi.MP_ERR_NAME

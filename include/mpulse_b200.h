@@ -408,6 +408,40 @@ int mp_initialize(mp_ctx *ctx, const mp_init *init);
  * it and its two neighbours in *position.  field: "Ex".."Bz". */
 int mp_follow_max(mp_ctx *ctx, const char *field, int dim, const int pos[3], int *ipos, double *position);
 
+/* HDF5 field dumps: the output of MPulse's "fielddiag" (FieldDiag,
+ * src/fielddiag.cpp:17-24 and src/diagnostic.t:1-30) through HDFostream
+ * (src/hdfstream.cpp:189-212, src/hdfstream.t:87-187), written from the device
+ * state by this library's own HDF5 encoder (HDF5 is not a dependency): the
+ * version 0 superblock, the root group as a symbol table, one contiguous
+ * dataset of IEEE doubles per field.
+ *
+ * mp_diag_file_name: DiagnosticInterface::parsedFileName
+ * (src/diagnostic.cpp:52-70): pattern with its first "#p" replaced by proc_id
+ * and its first "#t" by time, into out (n bytes).
+ *
+ * mp_hdf5_create: creates (truncates) the file mp_diag_file_name names.
+ * mp_hdf5_write_field: adds the field `name` of ctx (any name mp_download
+ * accepts that has the full-grid plane layout) as the next dataset, named as
+ * HDFstream::getNextBlockName names them after HDFostream::open
+ * (src/hdfstream.cpp:70-81, :189-212): "data0", "data1", "data2", ...; the
+ * dataset is MPulse's full grid with its ghost
+ * cells (x / y ghosts are the periodic images), dims {nz+2, ny+2, nx+2}: the
+ * element of MPulse cell (i, j, k) is dataset[k][j][i], as the reversed dims
+ * of src/hdfstream.t:110 make it.  Synchronises ctx's stream.  At most 256
+ * datasets per file.  "fielddiag" with append = "y" keeps one file and adds a
+ * dataset per output step; with "n" it creates a file per output step.
+ * mp_hdf5_close: writes the file's metadata and closes it (a file that is
+ * not closed is not a valid HDF5 file). */
+typedef struct mp_hdf5 mp_hdf5;
+int mp_diag_file_name(const char *pattern, int proc_id, long long time, char *out, size_t n);
+int mp_hdf5_create(const char *pattern, int proc_id, long long time, mp_hdf5 **out);
+int mp_hdf5_write_field(mp_hdf5 *file, mp_ctx *ctx, const char *name);
+/* Adds a host array of doubles with dims {dims[0], dims[1], dims[2]}, C
+ * order (dims[2] fastest), as the next dataset (what mp_hdf5_write_field
+ * writes after assembling the grid). */
+int mp_hdf5_write_grid(mp_hdf5 *file, const double *data, const size_t dims[3]);
+int mp_hdf5_close(mp_hdf5 *file);
+
 /* Checkpoint / restart of the whole device state: the six fields, the PLRC
  * accumulators, the CPML psi of every face and the time (the injector state
  * is a function of the time).  The buffer is opaque, in the device precision,

@@ -1302,6 +1302,15 @@ long long mp_launch_count(mp_ctx *c) { return c ? c->launches : -1; }
 
 namespace mpb {
 void set_global_error(const char *msg) { snprintf(g_create_err, sizeof g_create_err, "%s", msg); }
+
+// The grid of a context (for the HDF5 writer of mp_hdf5.cu).
+int ctx_grid(const mp_ctx *c, int *nx, int *ny, int *nz) {
+  if (!c) return MP_ERR_INVALID;
+  *nx = c->cfg.nx;
+  *ny = c->cfg.ny;
+  *nz = c->cfg.nz;
+  return MP_OK;
+}
 }  // namespace mpb
 
 extern "C" {

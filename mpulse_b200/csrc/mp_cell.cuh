@@ -87,9 +87,20 @@ __device__ __forceinline__ double rcp_pos(double d) {
   return r;
 }
 
+// The same with one Newton-Raphson step (relative error about 1e-14), for
+// the FP32 form, whose results are rounded to single precision.
+__device__ __forceinline__ double rcp_pos1(double d) {
+  if (!(d > 1e-30 && d < 1e30)) return 1.0 / d;
+  const double r = (double)__fdividef(1.0f, (float)d);
+  return fma(r, fma(-d, r, 1.0), r);
+}
+
 // Newton solve of |E| + A |E|^3 = C, FDTD_PLRCNonlinCore::plrcStepD
 // (fdtd_plrc.cpp:406-419), in FP64 whatever the field precision; capped at
-// maxit iterations.  Adds the iterations it ran to *iters.
+// maxit iterations.  Adds the iterations it ran to *iters.  FP32 = true: the
+// reciprocal of each step to about 1e-14 (rcp_pos1), enough for a result
+// rounded to single precision.
+template <bool FP32 = false>
 __device__ __forceinline__ double kerr_newton(double E, double A, double C, double tol, int maxit,
                                               int *status, unsigned *iters) {
   double Eold;
@@ -97,7 +108,8 @@ __device__ __forceinline__ double kerr_newton(double E, double A, double C, doub
   do {
     Eold = E;
     const double E2 = E * E;
-    E = (2.0 * A * E2 * E + C) * rcp_pos(3.0 * A * E2 + 1.0);
+    const double d = 3.0 * A * E2 + 1.0;
+    E = (2.0 * A * E2 * E + C) * (FP32 ? rcp_pos1(d) : rcp_pos(d));
     ++it;
   } while (fabs(E - Eold) > tol && it < maxit);
   if (fabs(E - Eold) > tol) atomicAdd(status + ST_NEWTON, 1);
@@ -420,12 +432,22 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       ezn = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ez, dt_mul(dt, dtl, cbz + jz) + Pz), lc.inv_denom,
                           lc.inv_denom_lo);
     } else {
-      const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
-      const T f = lc.numer + lc.chi * T(E2);
+      // |E^n|^2: in FP64 for the FP64 form; the FP32 form needs it only for
+      // the single-precision Kerr term and the start of the Newton solve
+      double E2;
+      T E2t;
+      if (sizeof(T) == 4) {
+        E2t = ex * ex + ey * ey + ez * ez;
+        E2 = E2t;
+      } else {
+        E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
+        E2t = T(E2);
+      }
+      const T f = lc.numer + lc.chi * E2t;
       T cx, cy, cz;
       if (sizeof(T) == 4) {
         // (numer + chi |E|^2) E + dt u + P with the compensated numer and dt
-        const T kf = lc.chi * T(E2);
+        const T kf = lc.chi * E2t;
         cx = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ex, fma(kf, ex, dt_mul(dt, dtl, cbx + jx) + Px)),
                            lc.inv_denom, lc.inv_denom_lo);
         cy = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ey, fma(kf, ey, dt_mul(dt, dtl, cby + jy) + Py)),
@@ -451,13 +473,14 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
         if (sizeof(T) == 4 && C2 > 1e-30 && C2 < 1e30) {
           rC = (double)rsqrtf((float)C2);
           rC = rC * fma(-0.5 * C2, rC * rC, 1.5);
-          E0 = (double)sqrtf((float)E2);
+          E0 = (double)sqrtf((float)E2t);
         } else {
           rC = rsqrt(C2);
           E0 = E2 > 0 ? E2 * rsqrt(E2) : 0.0;
         }
         const double C = C2 * rC;
-        const double E = kerr_newton(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status, &kc.iters);
+        const double E = kerr_newton<sizeof(T) == 4>(E0, lc.chi_over_denom, C, p.newton_tol, p.newton_max, p.status,
+                                                      &kc.iters);
         ++kc.solves;
         const double sc = E * rC;
         exn = T(sc * cx);

@@ -27,6 +27,7 @@ EXPORTED = (
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
     "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_state_size", "mp_save_state",
     "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max", "mp_kerr_counts",
+    "mp_diag_file_name", "mp_hdf5_create", "mp_hdf5_write_field", "mp_hdf5_write_grid", "mp_hdf5_close",
 )
 
 _lib = None
@@ -103,10 +104,84 @@ def lib():
     L.mp_follow_max.restype = C.c_int
     L.mp_kerr_counts.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.mp_kerr_counts.restype = C.c_int
+    L.mp_diag_file_name.argtypes = [cp, C.c_int, C.c_longlong, C.c_char_p, sz]
+    L.mp_diag_file_name.restype = C.c_int
+    L.mp_hdf5_create.argtypes = [cp, C.c_int, C.c_longlong, C.POINTER(vp)]
+    L.mp_hdf5_create.restype = C.c_int
+    L.mp_hdf5_write_field.argtypes = [vp, vp, cp]
+    L.mp_hdf5_write_field.restype = C.c_int
+    L.mp_hdf5_write_grid.argtypes = [vp, dp, C.POINTER(sz)]
+    L.mp_hdf5_write_grid.restype = C.c_int
+    L.mp_hdf5_close.argtypes = [vp]
+    L.mp_hdf5_close.restype = C.c_int
     L.mp_create_error.argtypes = []
     L.mp_create_error.restype = C.c_char_p
     _lib = L
     return L
+
+
+def _global_error() -> str:
+    buf = C.create_string_buffer(512)
+    lib().mp_last_error(None, buf, 512)
+    return buf.value.decode()
+
+
+def diag_file_name(pattern: str, proc_id: int, time: int) -> str:
+    """DiagnosticInterface::parsedFileName (diagnostic.cpp:52-70) through
+    mp_diag_file_name."""
+    out = C.create_string_buffer(len(pattern) + 64)
+    rc = lib().mp_diag_file_name(pattern.encode(), proc_id, time, out, len(out))
+    if rc != abi.MP_OK:
+        raise MPulseError(rc, _global_error())
+    return out.value.decode()
+
+
+class Hdf5File:
+    """One HDF5 output file (mp_hdf5_create ... mp_hdf5_close), the file of
+    an HDFostream: datasets "data0", "data1", ... in the order written."""
+
+    def __init__(self, pattern: str, proc_id: int = 0, time: int = 0):
+        self.name = diag_file_name(pattern, proc_id, time)
+        self._h = C.c_void_p()
+        rc = lib().mp_hdf5_create(pattern.encode(), proc_id, time, C.byref(self._h))
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, _global_error())
+
+    def write_field(self, sim: "Simulation", name: str):
+        """FieldDiag::write: the field `name` of sim as the next dataset."""
+        rc = lib().mp_hdf5_write_field(self._h, sim._h, name.encode())
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, sim.last_error() or _global_error())
+
+    def write_grid(self, a):
+        """A 3-D host array (C order) as the next dataset."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        dims = (C.c_size_t * 3)(*a.shape)
+        rc = lib().mp_hdf5_write_grid(self._h, _dptr(a), dims)
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, _global_error())
+
+    def close(self):
+        if self._h:
+            rc = lib().mp_hdf5_close(self._h)
+            self._h = None
+            if rc != abi.MP_OK:
+                raise MPulseError(rc, _global_error())
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def write_hdf5_arrays(pattern: str, arrays, proc_id: int = 0, time: int = 0) -> str:
+    """Writes 3-D host arrays (C order) as the datasets "data0", "data1", ...
+    of one HDF5 file (mp_hdf5_write_grid); returns the file name."""
+    with Hdf5File(pattern, proc_id, time) as f:
+        for a in arrays:
+            f.write_grid(a)
+    return f.name
 
 
 def library_defaults() -> abi.Config:
@@ -252,6 +327,17 @@ class Simulation:
         J = C.c_double()
         self._check(lib().mp_adjoint(self._h, C.byref(adj), C.byref(J), _dptr(g[0]), _dptr(g[1]), _dptr(g[2])))
         return J.value, {name: a.reshape(shape) for name, a in zip(abi.DESIGN_NAMES, g)}
+
+    # -- HDF5 field dumps (FieldDiag through HDFostream)
+    def write_hdf5(self, pattern: str, fields, proc_id: int = 0, time: int | None = None) -> str:
+        """Writes `fields` of the device state to one HDF5 file named by
+        `pattern` after the #p / #t substitution with proc_id and time (the
+        context's time by default); returns the file name."""
+        time = self.time if time is None else time
+        with Hdf5File(pattern, proc_id, time) as f:
+            for n in fields:
+                f.write_field(self, n)
+        return f.name
 
     # -- checkpoint / restart
     def save_state(self) -> bytes:

@@ -395,7 +395,9 @@ void build_params(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const std::vector<s
   bp.status = c->d_status;
   ep.n_field = bp.n_field = (long long)c->fcount;
   ep.n_psi = (long long)c->psi_cells;
-  // planes per block: enough blocks to fill 148 SMs several times over
+  // planes per block of the scalar B half (and a default the global-load E
+  // half replaces with its own, launch_e_np): enough blocks to fill 148 SMs
+  // several times over
   const long long blocks_xy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
   const long long target = 148LL * 8;
   const int ne = ep.k_last - ep.k_first + 1, nb = bp.k_last - bp.k_first + 1;

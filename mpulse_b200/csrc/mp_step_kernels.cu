@@ -51,6 +51,26 @@
 #ifndef MPB_B_MIN_THREADS
 #define MPB_B_MIN_THREADS 768
 #endif
+// E half z-chunks: planes per block chosen for about this many blocks of
+// 32 x MPB_E_BLOCK_Y columns per SM, so that the last, partly filled wave of
+// blocks is a small part of the launch, and at least MPB_E_MIN_PLANES planes
+// per block (the z-march carries the plane below in registers).  Measured on
+// the 256x256x512 PLRC + Kerr workload with the pulse in the Kerr medium
+// (FP32, E half): 103 planes per block (2560 blocks, 2.2 waves of the 1184
+// resident) 0.847 ms, 47 / 32 / 23 / 16 / 8 planes 0.774 / 0.772 / 0.757 /
+// 0.769 / 0.774 ms; blocks per SM 64 / 80 / 112: 0.765 / 0.758 / 0.753 ms.
+// FP64 (768 resident threads), 103 planes 1.695 ms, 24 / 48 / 80 blocks per
+// SM 1.632 / 1.563 / 1.540 ms.  On the 96^3 adjoint workload the forward run
+// takes the same time with at least 1, 2, 4 or 8 planes per block (±3%).
+#ifndef MPB_E_BLOCKS_PER_SM_F
+#define MPB_E_BLOCKS_PER_SM_F 80
+#endif
+#ifndef MPB_E_BLOCKS_PER_SM_D
+#define MPB_E_BLOCKS_PER_SM_D 80
+#endif
+#ifndef MPB_E_MIN_PLANES
+#define MPB_E_MIN_PLANES 2
+#endif
 // B half: two cells per thread with vector loads along x where nx allows,
 // with its own occupancy and z-chunks (half the threads), per precision.
 // Measured on the 256x256x512 workload (FP32, B half): scalar kernel 0.440
@@ -485,13 +505,18 @@ __global__ void __launch_bounds__(32 * MPB_B_BLOCK_Y,
 template <typename T, int MODE, bool DESIGN, bool PLASMA = false>
 static cudaError_t launch_e_np(const EParams<T> &p, int np, cudaStream_t st) {
   const int nk = p.k_last - p.k_first + 1;
-  const dim3 g((p.nx + 31) / 32, (p.ny + MPB_E_BLOCK_Y - 1) / MPB_E_BLOCK_Y, (nk + p.kchunk - 1) / p.kchunk),
+  const long long bxy = (long long)((p.nx + 31) / 32) * ((p.ny + MPB_E_BLOCK_Y - 1) / MPB_E_BLOCK_Y);
+  const long long per_sm = sizeof(T) == 4 ? MPB_E_BLOCKS_PER_SM_F : MPB_E_BLOCKS_PER_SM_D;
+  const long long chunks = std::max(1LL, (148LL * per_sm + bxy - 1) / bxy);
+  EParams<T> q = p;
+  q.kchunk = int(std::min<long long>(nk, std::max<long long>(MPB_E_MIN_PLANES, (nk + chunks - 1) / chunks)));
+  const dim3 g((p.nx + 31) / 32, (p.ny + MPB_E_BLOCK_Y - 1) / MPB_E_BLOCK_Y, (nk + q.kchunk - 1) / q.kchunk),
       b(32, MPB_E_BLOCK_Y, 1);
   switch (np) {
-    case 0: e_half_kernel<T, MODE, 0, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
-    case 1: e_half_kernel<T, MODE, 1, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
-    case 2: e_half_kernel<T, MODE, 2, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
-    default: e_half_kernel<T, MODE, 3, DESIGN, PLASMA><<<g, b, 0, st>>>(p); break;
+    case 0: e_half_kernel<T, MODE, 0, DESIGN, PLASMA><<<g, b, 0, st>>>(q); break;
+    case 1: e_half_kernel<T, MODE, 1, DESIGN, PLASMA><<<g, b, 0, st>>>(q); break;
+    case 2: e_half_kernel<T, MODE, 2, DESIGN, PLASMA><<<g, b, 0, st>>>(q); break;
+    default: e_half_kernel<T, MODE, 3, DESIGN, PLASMA><<<g, b, 0, st>>>(q); break;
   }
   return cudaGetLastError();
 }

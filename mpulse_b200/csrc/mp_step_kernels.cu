@@ -78,7 +78,11 @@
 // 0.354 ms; two cells per thread (float2) with 768 / 1024 / 1280 / 1536
 // threads 0.335 / 0.293 / 0.304 / 0.302 ms, 1024 threads and 32 / 48 blocks
 // per SM 0.290 / 0.285 ms (32 x 2 blocks: 0.284 ms, 32 x 8: 0.307 ms).  FP64 (double2), B half with 512 / 640 / 768 / 1024 threads:
-// 0.553 / 0.488 / 0.538 / 0.560 ms.
+// 0.553 / 0.488 / 0.538 / 0.560 ms.  Re-measured with the pulse in the Kerr
+// medium and the E half's z-chunks for 80 blocks per SM: FP32 48 / 80 / 128
+// blocks per SM 0.295 / 0.281 / 0.286 ms, FP64 24 / 48 / 80 blocks per SM
+// 0.510 / 0.495 / 0.468 ms; at least 4 instead of 8 planes per block: no
+// change.
 #ifndef MPB_B_VECTOR
 #define MPB_B_VECTOR 1
 #endif
@@ -89,10 +93,13 @@
 #define MPB_BV_MIN_THREADS_D 640
 #endif
 #ifndef MPB_BV_BLOCKS_PER_SM_F
-#define MPB_BV_BLOCKS_PER_SM_F 48
+#define MPB_BV_BLOCKS_PER_SM_F 80
 #endif
 #ifndef MPB_BV_BLOCKS_PER_SM_D
-#define MPB_BV_BLOCKS_PER_SM_D 24
+#define MPB_BV_BLOCKS_PER_SM_D 80
+#endif
+#ifndef MPB_BV_MIN_PLANES
+#define MPB_BV_MIN_PLANES 8
 #endif
 // B half, scalar kernel: issue the next plane's loads before the current
 // plane's arithmetic.
@@ -556,7 +563,7 @@ cudaError_t launch_b_half(const BParams<T> &p, cudaStream_t st) {
     const long long bxy = (long long)(tx / 32) * ((p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y);
     const long long chunks = std::max(1LL, (148LL * per_sm + bxy - 1) / bxy);
     BParams<T> q = p;
-    q.kchunk = int(std::max(8LL, (nk + chunks - 1) / chunks));
+    q.kchunk = int(std::max<long long>(MPB_BV_MIN_PLANES, (nk + chunks - 1) / chunks));
     const dim3 g((tx + 31) / 32, (p.ny + MPB_B_BLOCK_Y - 1) / MPB_B_BLOCK_Y, (nk + q.kchunk - 1) / q.kchunk);
     b_half_vec_kernel<T><<<g, dim3(32, MPB_B_BLOCK_Y, 1), 0, st>>>(q);
     return cudaGetLastError();

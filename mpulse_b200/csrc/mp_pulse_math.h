@@ -60,14 +60,19 @@ MPB_HD cd cexp_(cd z) {
 }
 MPB_HD cd I_() { return cd(0.0, 1.0); }
 
-// w(z) for Im z >= 0 by Weideman's expansion; coef[0] is the highest power.
+// w(z) for Im z >= 0 by Weideman's expansion; coef[0] is the highest power:
+// with r = 1 / (L - iz) and Z = (L + iz) r, w = 2 p(Z) r^2 + r / sqrt(pi).
+// Re(L - iz) = L + Im z >= L, so r = conj(L - iz) / |L - iz|^2 needs one real
+// division and cannot overflow or underflow for any finite z of interest.
 MPB_HD cd faddeeva(cd z, const double *coef, double L) {
   const cd iz(-z.im, z.re);
   const cd Lmz = cd(L) - iz;
-  const cd Z = (cd(L) + iz) / Lmz;
+  const double den = 1.0 / (Lmz.re * Lmz.re + Lmz.im * Lmz.im);
+  const cd r(Lmz.re * den, -Lmz.im * den);
+  const cd Z = (cd(L) + iz) * r;
   cd p(coef[0]);
   for (int n = 1; n < kFaddeevaTerms; ++n) p = p * Z + coef[n];
-  return 2.0 * p / (Lmz * Lmz) + (1.0 / sqrt(M_PI)) / Lmz;
+  return (2.0 * p * r + (1.0 / sqrt(M_PI))) * r;
 }
 
 // Coefficients a_N .. a_1 (highest power first) and L = sqrt(N / sqrt 2):

@@ -109,8 +109,17 @@ cudaError_t launch_source_plane(const SourceEvalParams &q, T *v0, T *v1, cudaStr
 // The planes of `nsteps` consecutive steps in one launch: the values depend
 // only on Process::time, so step t0 + q's E-side pair goes to
 // out + (4 q + 0, 1) * plane and its H-side pair to out + (4 q + 2, 3) * plane.
+// The short-pulse closed forms are long FP64 expressions (about 240 registers
+// unbounded, one block of 256 threads per SM): asking for MPB_SRC_MIN_BLOCKS
+// blocks per SM trades spills for occupancy.  Measured on the 256 x 256 plane
+// of the PLRC + Kerr workload: 1 / 2 / 3 blocks per SM 0.042 / 0.025 / 0.022
+// ms per step; with the one-division Faddeeva function 2 / 3 / 4 blocks
+// 0.0196 / 0.0183 / 0.0194 ms.
+#ifndef MPB_SRC_MIN_BLOCKS
+#define MPB_SRC_MIN_BLOCKS 3
+#endif
 template <typename T>
-__global__ void __launch_bounds__(256) source_batch_kernel(const SourceEvalParams qe, const SourceEvalParams qh,
+__global__ void __launch_bounds__(256, MPB_SRC_MIN_BLOCKS) source_batch_kernel(const SourceEvalParams qe, const SourceEvalParams qh,
                                                           long long t0, T *out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;

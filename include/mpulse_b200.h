@@ -107,12 +107,22 @@ typedef enum mp_source_kind {
   MP_SOURCE_GAUSS_BEAM = 5      /* "gauss_inject"       gaussinject.cpp */
 } mp_source_kind;
 
-/* Kernel form of the step; all forms give bit-identical results.  GLOBAL reads
- * global memory directly (L1/L2 serve the neighbours); TMA stages each z-plane
- * in a shared-memory ring with TMA tile loads (needs nx a multiple of 32 and
- * ny of 8, else mp_create fails with MP_ERR_UNSUPPORTED); AUTO picks the form
- * measured fastest on B200, currently GLOBAL. */
-typedef enum mp_staging { MP_STAGING_AUTO = 0, MP_STAGING_GLOBAL = 1, MP_STAGING_TMA = 2 } mp_staging;
+/* Kernel form of the step.  All forms run the same cell arithmetic and agree
+ * to the last bit, or within rounding (FP64: 1e-14 relative) where a kernel's
+ * own vector code leaves a multiply-add to the compiler.  GLOBAL reads
+ * global memory directly (L1/L2 serve the neighbours), one kernel per half
+ * step; TMA stages each z-plane in a shared-memory ring with TMA tile loads
+ * (needs nx a multiple of 32 and ny of 8, else mp_create fails with
+ * MP_ERR_UNSUPPORTED); FUSED runs both half steps of a tile of columns in one
+ * z-march and the cells on the tiles' edges in a second, small kernel (not
+ * with a design region or the plasma plug-ins: MP_ERR_UNSUPPORTED); AUTO
+ * picks the form measured fastest on B200 for the configuration. */
+typedef enum mp_staging {
+  MP_STAGING_AUTO = 0,
+  MP_STAGING_GLOBAL = 1,
+  MP_STAGING_TMA = 2,
+  MP_STAGING_FUSED = 3
+} mp_staging;
 
 /* One Lorentz pole: MPulse's L<n>eps, L<n>delta, L<n>Om2
  * (src/fdtd_plrc.t:419-429, src/fdtd_plrc.h:85-90). */

@@ -40,7 +40,7 @@ MP_FP64, MP_FP32 = 0, 1
 MP_SOLVER_PLAIN, MP_SOLVER_NL, MP_SOLVER_PLRC_LIN, MP_SOLVER_PLRC_NONLIN = 0, 1, 2, 3
 MP_BOUNDARY_PERIODIC, MP_BOUNDARY_XY_PERIODIC = 0, 1
 MP_CPML_NONE, MP_CPML_ALL, MP_CPML_Z = 0, 1, 2
-MP_STAGING_AUTO, MP_STAGING_GLOBAL, MP_STAGING_TMA = 0, 1, 2
+MP_STAGING_AUTO, MP_STAGING_GLOBAL, MP_STAGING_TMA, MP_STAGING_FUSED = 0, 1, 2, 3
 (MP_SOURCE_NONE, MP_SOURCE_PLANE_WAVE, MP_SOURCE_PLANE_GAUSS,
  MP_SOURCE_SHORT_PULSE, MP_SOURCE_FOCUSED_PULSE, MP_SOURCE_GAUSS_BEAM) = range(6)
 

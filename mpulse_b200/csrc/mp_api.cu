@@ -42,6 +42,8 @@ template <typename T>
 cudaError_t launch_e_half_tma(const EParams<T> &, const ETmaMaps &, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_b_half_tma(const BParams<T> &, const BTmaMaps &, cudaStream_t);
+template <typename T>
+cudaError_t launch_step_fused(const EParams<T> &, const BParams<T> &, int, int, int, cudaStream_t);
 void tma_boxes(int esz, int e_box[7][2], int b_box[6][2]);
 #ifndef MPB_ADJ_E_BPSM
 #define MPB_ADJ_E_BPSM 8
@@ -139,7 +141,8 @@ struct mp_ctx {
   BParams<float> bpf;
   EParams<double> epd;
   BParams<double> bpd;
-  bool tma = false;  // TMA-staged kernels in use
+  bool tma = false;    // TMA-staged kernels in use
+  bool fused = false;  // the fused step kernel and its border kernel in use
   ETmaMaps etma;
   BTmaMaps btma;
   // design region (mp_config.design_box): FP64 maps eps, Delta-eps factor, chi factor
@@ -258,7 +261,8 @@ int validate(const mp_config *c) {
     if (!(q.eps > 0)) return set_err(nullptr, MP_ERR_INVALID, "source %d: eps must be positive", s);
   }
   if (c->newton_max_iter < 1) return set_err(nullptr, MP_ERR_INVALID, "newton_max_iter must be >= 1");
-  if (c->staging != MP_STAGING_AUTO && c->staging != MP_STAGING_GLOBAL && c->staging != MP_STAGING_TMA)
+  if (c->staging != MP_STAGING_AUTO && c->staging != MP_STAGING_GLOBAL && c->staging != MP_STAGING_TMA &&
+      c->staging != MP_STAGING_FUSED)
     return set_err(nullptr, MP_ERR_INVALID, "unknown staging %d", c->staging);
   const int *db = c->design_box;
   if (db[0] <= db[1]) {
@@ -269,14 +273,14 @@ int validate(const mp_config *c) {
     if (db[4] < c->medium_z0 || db[5] > c->medium_z1)
       return set_err(nullptr, MP_ERR_INVALID, "design box outside the medium planes %d..%d", c->medium_z0,
                      c->medium_z1);
-    if (c->staging == MP_STAGING_TMA)
+    if (c->staging == MP_STAGING_TMA || c->staging == MP_STAGING_FUSED)
       return set_err(nullptr, MP_ERR_UNSUPPORTED, "design regions use the global-load kernels (staging GLOBAL/AUTO)");
   }
   if (c->plasma || c->plasma_current) {
     if (!plrc) return set_err(nullptr, MP_ERR_INVALID, "the plasma plug-ins belong to the PLRC solvers (fdtd_plrc.t:431-436)");
     if (c->plasma && (c->plasma_k < 1 || c->plasma_k > 64))
       return set_err(nullptr, MP_ERR_INVALID, "plasma K %d outside 1..64", c->plasma_k);
-    if (c->staging == MP_STAGING_TMA)
+    if (c->staging == MP_STAGING_TMA || c->staging == MP_STAGING_FUSED)
       return set_err(nullptr, MP_ERR_UNSUPPORTED, "the plasma plug-ins use the global-load kernels (staging GLOBAL/AUTO)");
     if (db[0] <= db[1]) return set_err(nullptr, MP_ERR_UNSUPPORTED, "the plasma plug-ins and a design region together");
   }
@@ -789,6 +793,7 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   // kernels (E 0.92 ms, B 0.47 ms per launch) beat the TMA-staged ones
   // (E 1.12 ms, B 0.61 ms), whose 12 small tile copies per plane and block
   // serialise in the copy engine.
+  c->fused = g.staging == MP_STAGING_FUSED;
   if (g.staging == MP_STAGING_TMA) {
     if (!setup_tma(c)) return fail(set_err(c, MP_ERR_UNSUPPORTED, "TMA tensor maps could not be encoded"));
     // TMA kernels: two resident blocks per SM; about four waves of blocks so
@@ -999,12 +1004,16 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
       }
       NvtxRange nv("mp step");
       if (tm) cudaEventRecord(tm->ev[0], c->stream);
-      e = c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
-                 : launch_e_half<T>(ep, c->mode, c->np, c->stream);
+      // (the fused form: its step kernel in the E slot, the border kernel in the B slot)
+      e = c->fused ? launch_step_fused<T>(ep, bp, c->mode, c->np, 1, c->stream)
+          : c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
+                   : launch_e_half<T>(ep, c->mode, c->np, c->stream);
       if (e != cudaSuccess) return cuda_err(c, e, "E half-step kernel");
       c->launches++;
       if (tm) cudaEventRecord(tm->ev[1], c->stream);
-      e = c->tma ? launch_b_half_tma<T>(bp, c->btma, c->stream) : launch_b_half<T>(bp, c->stream);
+      e = c->fused ? launch_step_fused<T>(ep, bp, c->mode, c->np, 2, c->stream)
+          : c->tma ? launch_b_half_tma<T>(bp, c->btma, c->stream)
+                   : launch_b_half<T>(bp, c->stream);
       if (e != cudaSuccess) return cuda_err(c, e, "B half-step kernel");
       c->launches++;
       if (tm) {

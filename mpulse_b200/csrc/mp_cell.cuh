@@ -171,6 +171,31 @@ __device__ __forceinline__ T inv_denom_mul(T x, T idn, T idn_lo) {
   return sizeof(T) == 4 ? fma(x, idn, x * idn_lo) : x * idn;
 }
 
+// Sums of two products spelled out as one FMA: a b + c d, a b - c d, and
+// a^2 + b^2 + c^2.  Left to the compiler, either product of such a sum may be
+// fused, and the choice differs between kernels that inline the same cell
+// code (it did between the fused step kernel, whose neighbours come from
+// shared memory, and the half-step kernels); spelled out, every kernel form
+// rounds alike.  A lone a b + c is fused the same way everywhere.
+template <typename T>
+__device__ __forceinline__ T fma_pp(T a, T b, T c, T d) {
+  return fma(a, b, c * d);
+}
+template <typename T>
+__device__ __forceinline__ T fma_pm(T a, T b, T c, T d) {
+  return fma(a, b, -(c * d));
+}
+template <typename T>
+__device__ __forceinline__ T sq3(T a, T b, T c) {
+  return fma(c, c, fma(b, b, a * a));
+}
+
+// e + dt u with the FP32 form's compensated step; in FP64 one FMA.
+template <typename T>
+__device__ __forceinline__ T add_dt(T e, T dt, T dt_lo, T u) {
+  return sizeof(T) == 4 ? e + fma(dt, u, dt_lo * u) : fma(dt, u, e);
+}
+
 // The plasma plug-ins at one cell, from E^n (before the E update):
 // PlasmaDensity::stepScheme (plasmadensity.cpp:18-49) gives the new density
 // and the conductivity Sigma = mpa Wion I^(K-1) of this step (Sigma is reset
@@ -189,18 +214,18 @@ __device__ __forceinline__ void plasma_cell(const EParams<T> &p, T ex, T ey, T e
   pc.rho = rho;
   pc.sig = T(0);
   if (p.pl_density) {
-    const T I = ex * ex + ey * ey + ez * ez;
+    const T I = sq3(ex, ey, ez);
     T IKm = T(1);  // util.h ipow: K - 1 products
     for (int q = 0; q < p.pl_km; ++q) IKm *= I;
     const T IK = I * IKm;
-    pc.rho = (rho * (T(1) + p.pl_n * I) + p.pl_m * IK) / (T(1) - p.pl_n * I);
+    pc.rho = fma_pp(rho, T(1) + p.pl_n * I, p.pl_m, IK) / (T(1) - p.pl_n * I);
     pc.sig = T(0.5) * (p.pl_w * IKm) * p.dt;
   }
   if (p.pl_current) {
     const T r = pc.rho + p.pl_rho_bg;
-    pc.j[0] = (j0 * p.pl_gdtn - p.pl_emdt * ex * r) / p.pl_gdtd;
-    pc.j[1] = (j1 * p.pl_gdtn - p.pl_emdt * ey * r) / p.pl_gdtd;
-    pc.j[2] = (j2 * p.pl_gdtn - p.pl_emdt * ez * r) / p.pl_gdtd;
+    pc.j[0] = fma_pm(j0, p.pl_gdtn, p.pl_emdt * ex, r) / p.pl_gdtd;
+    pc.j[1] = fma_pm(j1, p.pl_gdtn, p.pl_emdt * ey, r) / p.pl_gdtd;
+    pc.j[2] = fma_pm(j2, p.pl_gdtn, p.pl_emdt * ez, r) / p.pl_gdtd;
   } else {
     pc.j[0] = pc.j[1] = pc.j[2] = T(0);
   }
@@ -342,8 +367,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     if (dim == 2) { d0 = -(v.by - v.by_km); d1 = v.bx - v.bx_km; }
     else if (dim == 0) { d0 = -(v.bz - v.bz_xm); d1 = v.by - v.by_xm; }
     else { d0 = -(v.bx - v.bx_ym); d1 = v.bz - v.bz_ym; }
-    cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
-    cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+    cp0[f] = fma_pp(cb[f], cp0[f], cc[f], d0);
+    cp1[f] = fma_pp(cb[f], cp1[f], cc[f], d1);
     if (dim == 2) { jx += cp0[f]; jy += cp1[f]; }
     else if (dim == 0) { jy += cp0[f]; jz += cp1[f]; }
     else { jz += cp0[f]; jx += cp1[f]; }
@@ -361,22 +386,22 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
   }
 
   // curl_kappa B (fdtd_plrc.cpp:207-244)
-  const T cbx = (v.bz - v.bz_ym) * iky - (v.by - v.by_km) * ikz;
-  const T cby = (v.bx - v.bx_km) * ikz - (v.bz - v.bz_xm) * ikx;
-  const T cbz = (v.by - v.by_xm) * ikx - (v.bx - v.bx_ym) * iky;
+  const T cbx = fma_pm(v.bz - v.bz_ym, iky, v.by - v.by_km, ikz);
+  const T cby = fma_pm(v.bx - v.bx_km, ikz, v.bz - v.bz_xm, ikx);
+  const T cbz = fma_pm(v.by - v.by_xm, ikx, v.bx - v.bx_ym, iky);
   const T ex = v.ex, ey = v.ey, ez = v.ez;
 
   const T dtl = p.dt_lo;
   if (MODE == MODE_PLAIN) {
-    exn = ex + dt_mul(dt, dtl, cbx);
-    eyn = ey + dt_mul(dt, dtl, cby);
-    ezn = ez + dt_mul(dt, dtl, cbz);
+    exn = add_dt(ex, dt, dtl, cbx);
+    eyn = add_dt(ey, dt, dtl, cby);
+    ezn = add_dt(ez, dt, dtl, cbz);
   } else if (MODE == MODE_NL) {
-    const double E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
+    const double E2 = sq3((double)ex, (double)ey, (double)ez);
     const T f = T(p.eps_d + p.chi_d * E2);
-    const T Dx = f * ex + dt_mul(dt, dtl, cbx), Dy = f * ey + dt_mul(dt, dtl, cby),
-            Dz = f * ez + dt_mul(dt, dtl, cbz);
-    const double D2 = (double)Dx * Dx + (double)Dy * Dy + (double)Dz * Dz;
+    const T Dx = fma(f, ex, dt_mul(dt, dtl, cbx)), Dy = fma(f, ey, dt_mul(dt, dtl, cby)),
+            Dz = fma(f, ez, dt_mul(dt, dtl, cbz));
+    const double D2 = sq3((double)Dx, (double)Dy, (double)Dz);
     if (D2 > 0) {
       const double rD = rsqrt(D2);  // as in the PLRC Kerr update below
       const double D = D2 * rD;
@@ -394,13 +419,13 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
     // background: no poles, no Kerr term
     if (PLASMA && p.pl_density) {
       const T nb = p.eps_bg - pc->sig, ib = T(1) / (p.eps_bg + pc->sig);
-      exn = (nb * ex + dt_mul(dt, dtl, cbx + jx)) * ib;
-      eyn = (nb * ey + dt_mul(dt, dtl, cby + jy)) * ib;
-      ezn = (nb * ez + dt_mul(dt, dtl, cbz + jz)) * ib;
+      exn = fma(nb, ex, dt_mul(dt, dtl, cbx + jx)) * ib;
+      eyn = fma(nb, ey, dt_mul(dt, dtl, cby + jy)) * ib;
+      ezn = fma(nb, ez, dt_mul(dt, dtl, cbz + jz)) * ib;
     } else {
-      exn = (p.eps_bg * ex + dt_mul(dt, dtl, cbx + jx)) * p.inv_eps_bg;
-      eyn = (p.eps_bg * ey + dt_mul(dt, dtl, cby + jy)) * p.inv_eps_bg;
-      ezn = (p.eps_bg * ez + dt_mul(dt, dtl, cbz + jz)) * p.inv_eps_bg;
+      exn = fma(p.eps_bg, ex, dt_mul(dt, dtl, cbx + jx)) * p.inv_eps_bg;
+      eyn = fma(p.eps_bg, ey, dt_mul(dt, dtl, cby + jy)) * p.inv_eps_bg;
+      ezn = fma(p.eps_bg, ez, dt_mul(dt, dtl, cbz + jz)) * p.inv_eps_bg;
     }
   } else {
     T Px = T(0), Py = T(0), Pz = T(0);
@@ -416,8 +441,8 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
           const T ai = lc.pD[n][1] * e3[c] + q[n][c].y;
           P3[c] += ar;
           // psi <- dxi0 e + Crec psi~
-          q[n][c].x = lc.pxi[n][0] * e3[c] + (p.pC[n][0] * ar - p.pC[n][1] * ai);
-          q[n][c].y = lc.pxi[n][1] * e3[c] + (p.pC[n][0] * ai + p.pC[n][1] * ar);
+          q[n][c].x = fma(lc.pxi[n][0], e3[c], fma_pm(p.pC[n][0], ar, p.pC[n][1], ai));
+          q[n][c].y = fma(lc.pxi[n][1], e3[c], fma_pp(p.pC[n][0], ai, p.pC[n][1], ar));
         }
       }
       Px = P3[0];
@@ -437,10 +462,10 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       double E2;
       T E2t;
       if (sizeof(T) == 4) {
-        E2t = ex * ex + ey * ey + ez * ez;
+        E2t = sq3(ex, ey, ez);
         E2 = E2t;
       } else {
-        E2 = (double)ex * ex + (double)ey * ey + (double)ez * ez;
+        E2 = sq3((double)ex, (double)ey, (double)ez);
         E2t = T(E2);
       }
       const T f = lc.numer + lc.chi * E2t;
@@ -455,9 +480,9 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
         cz = inv_denom_mul(numer_mul_add(lc.numer, lc.numer_lo, ez, fma(kf, ez, dt_mul(dt, dtl, cbz + jz) + Pz)),
                            lc.inv_denom, lc.inv_denom_lo);
       } else {
-        cx = (f * ex + dt * (cbx + jx) + Px) * lc.inv_denom;
-        cy = (f * ey + dt * (cby + jy) + Py) * lc.inv_denom;
-        cz = (f * ez + dt * (cbz + jz) + Pz) * lc.inv_denom;
+        cx = fma(f, ex, fma(dt, cbx + jx, Px)) * lc.inv_denom;
+        cy = fma(f, ey, fma(dt, cby + jy, Py)) * lc.inv_denom;
+        cz = fma(f, ez, fma(dt, cbz + jz, Pz)) * lc.inv_denom;
       }
       // |c|, 1/|c| and the start |E^n| from reciprocal square roots: no FP64
       // square root or division here (equal to sqrt and / up to rounding).
@@ -467,7 +492,7 @@ __device__ __forceinline__ void e_cell(const EParams<T> &p, int i, int j, int k,
       // start |E^n| of the Newton solve in single precision (the solve
       // converges to the same root from any start near it); outside the
       // normal single-precision range it takes the FP64 path.
-      const double C2 = (double)cx * cx + (double)cy * cy + (double)cz * cz;
+      const double C2 = sq3((double)cx, (double)cy, (double)cz);
       if (C2 > 0) {
         double rC, E0;
         if (sizeof(T) == 4 && C2 > 1e-30 && C2 < 1e30) {
@@ -546,8 +571,8 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
     if (dim == 2) { d0 = v.ey_kp - v.ey; d1 = -(v.ex_kp - v.ex); }
     else if (dim == 0) { d0 = v.ez_xp - v.ez; d1 = -(v.ey_xp - v.ey); }
     else { d0 = v.ex_yp - v.ex; d1 = -(v.ez_yp - v.ez); }
-    cp0[f] = cb[f] * cp0[f] + cc[f] * d0;
-    cp1[f] = cb[f] * cp1[f] + cc[f] * d1;
+    cp0[f] = fma_pp(cb[f], cp0[f], cc[f], d0);
+    cp1[f] = fma_pp(cb[f], cp1[f], cc[f], d1);
     if (dim == 2) { mx += cp0[f]; my += cp1[f]; }
     else if (dim == 0) { my += cp0[f]; mz += cp1[f]; }
     else { mz += cp0[f]; mx += cp1[f]; }
@@ -560,9 +585,9 @@ __device__ __forceinline__ void b_cell(const BParams<T> &p, int i, int j, int k,
   }
 
   // ---- plrcStepB (fdtd_plrc.cpp:263-293)
-  bxn = v.bx + dt_mul(dt, p.dt_lo, (v.ey_kp - v.ey) * ikz - (v.ez_yp - v.ez) * iky + mx);
-  byn = v.by + dt_mul(dt, p.dt_lo, (v.ez_xp - v.ez) * ikx - (v.ex_kp - v.ex) * ikz + my);
-  bzn = v.bz + dt_mul(dt, p.dt_lo, (v.ex_yp - v.ex) * iky_bz - (v.ey_xp - v.ey) * ikx + mz);
+  bxn = add_dt(v.bx, dt, p.dt_lo, fma_pm(v.ey_kp - v.ey, ikz, v.ez_yp - v.ez, iky) + mx);
+  byn = add_dt(v.by, dt, p.dt_lo, fma_pm(v.ez_xp - v.ez, ikx, v.ex_kp - v.ex, ikz) + my);
+  bzn = add_dt(v.bz, dt, p.dt_lo, fma_pm(v.ex_yp - v.ex, iky_bz, v.ey_xp - v.ey, ikx) + mz);
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     if (!cin[f]) continue;

@@ -480,6 +480,19 @@ int mp_objective(mp_ctx *ctx, const mp_adjoint_config *adj, double *J);
 int mp_adjoint(mp_ctx *ctx, const mp_adjoint_config *adj, double *J, double *grad_eps,
                double *grad_deps_scale, double *grad_chi_scale);
 
+/* Reserves pinned host memory for mp_adjoint's checkpoints: as many buffers
+ * of one forward state each as fit in `bytes` (allocated and pinned now, which
+ * takes seconds for tens of GB; freed by the next call or mp_destroy; 0 frees
+ * them).  With a device budget (mem_budget, checkpoint_every = 0) and at least
+ * two such buffers, mp_adjoint may add a second level to its schedule: the
+ * first forward run copies the state at the start of every segment of L steps
+ * to host memory, and each segment is then reversed, last first, on the
+ * device schedule for L steps, starting from its host copy.  It does so when
+ * that runs fewer forward steps, counting each host copy as the steps that
+ * take as long.  The results are the same as with any other schedule.
+ * MP_ERR_NO_MEMORY when the host memory cannot be pinned (nothing is kept). */
+int mp_set_host_checkpoint_budget(mp_ctx *ctx, double bytes);
+
 /* Copies the message of the last failure (or "") into buf. */
 int mp_last_error(mp_ctx *ctx, char *buf, size_t n);
 

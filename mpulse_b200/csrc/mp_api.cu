@@ -18,14 +18,19 @@
 #include <nvtx3/nvToolsExt.h>  // header-only NVTX: ranges for Nsight timelines, no cost without a tool
 
 #include <algorithm>
+#include <cmath>
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <sys/mman.h>
 
 namespace mpb {
 template <typename T> cudaError_t launch_e_half(const EParams<T> &, int, int, cudaStream_t);
@@ -143,6 +148,7 @@ struct mp_ctx {
   BParams<double> bpd;
   bool tma = false;    // TMA-staged kernels in use
   bool fused = false;  // the fused step kernel and its border kernel in use
+  std::vector<void *> host_ckpt;  // pinned host buffers of one state each (mp_set_host_checkpoint_budget)
   ETmaMaps etma;
   BTmaMaps btma;
   // design region (mp_config.design_box): FP64 maps eps, Delta-eps factor, chi factor
@@ -1115,6 +1121,15 @@ int mp_create(const mp_config *cfg, mp_ctx **out) {
 
 const char *mp_create_error(void) { return g_create_err; }
 
+// The pinned host checkpoint buffers of mp_set_host_checkpoint_budget.
+static void free_host_ckpt(mp_ctx *c) {
+  for (void *p : c->host_ckpt) {
+    cudaHostUnregister(p);
+    std::free(p);
+  }
+  c->host_ckpt.clear();
+}
+
 void mp_destroy(mp_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
@@ -1136,6 +1151,7 @@ void mp_destroy(mp_ctx *c) {
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_kerr) cudaFreeHost(c->h_kerr);
   if (c->h_diag) cudaFreeHost(c->h_diag);
+  free_host_ckpt(c);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -1673,6 +1689,54 @@ bool plan_schedule(long long Tn, long long every, double budget, size_t S, size_
   return best >= 0;
 }
 
+// Two-level schedule under a device budget and a host budget: the first
+// forward run keeps the state at the start of every segment of L steps in
+// pinned host memory (one state of S bytes per segment), and each segment is
+// then reversed, last first, on the device schedule plan_schedule gives for L
+// steps, starting from its host copy.  Taken when its forward steps plus the
+// host copies (two per segment but the last, each counted as the steps that
+// take as long: a step moves about 2.5 S through HBM at 4 TB/s and costs at
+// least two launches of 10 us, a copy moves S through PCIe at 20 GB/s after
+// 20 us) are fewer than the steps of the device schedule alone.
+struct TwoLevel {
+  long long L = 0, nseg = 0, Kh = 0;
+  int slots = 0, nbuf = 1;
+};
+
+bool plan_two_level(long long Tn, double budget, double host_budget, size_t S, size_t H, long long one_level_steps,
+                    TwoLevel *out) {
+  if (!(host_budget > 0) || !(budget > 0) || S == 0) return false;
+  const long long host_slots = (long long)std::floor(host_budget / double(S));
+  if (host_slots < 2) return false;
+  const double t_step = std::max(2.5 * double(S) / 4e12, 20e-6), t_copy = double(S) / 20e9 + 20e-6;
+  const double copy_steps = t_copy / t_step;  // one host copy, in steps
+  bool found = false;
+  double best = double(one_level_steps);
+  // fewer, longer segments than the host allows when that is cheaper
+  for (long long nseg = host_slots; nseg >= 2; nseg = std::min(nseg - 1, (long long)(nseg * 0.8))) {
+    const long long L = (Tn + nseg - 1) / nseg;
+    const long long ns = (Tn + L - 1) / L;
+    if (ns < 2) continue;
+    long long Kh;
+    int slots, nbuf;
+    if (!plan_schedule(L, 0, budget, S, H, &Kh, &slots, &nbuf)) continue;
+    // first run up to the last segment, then every segment on its schedule
+    const long long last = Tn - (ns - 1) * L;
+    const double steps = double((ns - 1) * L) + double(ns - 1) * double(schedule_steps(L, Kh, slots)) +
+                         double(schedule_steps(last, Kh, slots)) + copy_steps * double(2 * ns - 1);
+    if (steps < best) {
+      best = steps;
+      out->L = L;
+      out->nseg = ns;
+      out->Kh = Kh;
+      out->slots = slots;
+      out->nbuf = nbuf;
+      found = true;
+    }
+  }
+  return found;
+}
+
 // The forward run and the reverse pass on the schedule of plan_schedule /
 // revolve: each chunk [n0, n1) is run forward from the live state or a
 // checkpoint keeping E (and, for the Sz objective, Bx and By on the plane) of
@@ -1696,6 +1760,17 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     return set_err(c, MP_ERR_NO_MEMORY,
                    "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
                    a->mem_budget, S, H);
+  // segments whose starts go to host memory, under a budget (not with an
+  // explicit checkpoint_every)
+  TwoLevel tl;
+  const bool two = a->checkpoint_every <= 0 && Kh < Tn &&
+                   plan_two_level(Tn, a->mem_budget, double(c->host_ckpt.size()) * double(S), S, H,
+                                  schedule_steps(Tn, Kh, slots), &tl);
+  if (two) {
+    Kh = tl.Kh;
+    slots = tl.slots;
+    nbuf = tl.nbuf;
+  }
   const long long K = Kh;
 
   DevBufs buf(c->stream);
@@ -1954,12 +2029,47 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     cur = (cur + 1) % nbuf;
     return MP_OK;
   };
-  if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
-  std::vector<int> free_slots;
-  for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+  int rc = MP_OK;
   long long live = 0;
-  int rc = revolve(0, Tn, 0, free_slots, K, ops, live);
-  if (rc != MP_OK) return rc;
+  if (!two) {
+    if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+    std::vector<int> free_slots;
+    for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+    rc = revolve(0, Tn, 0, free_slots, K, ops, live);
+    if (rc != MP_OK) return rc;
+  } else {
+    // the live state to / from the host copy of segment k, on the stream
+    auto host_copy = [&](long long k, bool save) -> cudaError_t {
+      size_t off = 0;
+      for (const auto &r : regions) {
+        char *hc = static_cast<char *>(c->host_ckpt[size_t(k)]) + off;
+        cudaError_t err = save ? cudaMemcpyAsync(hc, r.first, r.second, cudaMemcpyDeviceToHost, c->stream)
+                               : cudaMemcpyAsync(r.first, hc, r.second, cudaMemcpyHostToDevice, c->stream);
+        if (err != cudaSuccess) return err;
+        off += r.second;
+      }
+      return cudaSuccess;
+    };
+    // first run: the start of every segment to host memory
+    for (long long k = 0; k < tl.nseg; ++k) {
+      if ((e = host_copy(k, true)) != cudaSuccess) return cuda_err(c, e, "host checkpoint copy");
+      if (k + 1 < tl.nseg && (rc = ops.advance(k * tl.L, (k + 1) * tl.L)) != MP_OK) return rc;
+      live = k * tl.L + (k + 1 < tl.nseg ? tl.L : 0);
+    }
+    // segments last first, each from its host copy on the device schedule
+    for (long long k = tl.nseg - 1; k >= 0; --k) {
+      const long long a0 = k * tl.L, a1 = std::min(Tn, a0 + tl.L);
+      if (live != a0) {
+        if ((e = host_copy(k, false)) != cudaSuccess) return cuda_err(c, e, "host checkpoint restore");
+        c->time = t0 + a0;
+        live = a0;
+      }
+      if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+      std::vector<int> free_slots;
+      for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+      if ((rc = revolve(a0, a1, 0, free_slots, K, ops, live)) != MP_OK) return rc;
+    }
+  }
   if ((e = cudaStreamSynchronize(rs.s)) != cudaSuccess) return cuda_err(c, e, "adjoint");
   if ((e = copy_state(slots, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
   c->time = t0 + Tn;
@@ -1999,6 +2109,46 @@ int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_ep
   cudaSetDevice(c->cfg.device);
   double *g[3] = {grad_eps, grad_deps_scale, grad_chi_scale};
   return c->fp32 ? adjoint_impl<float>(c, c->epf, c->bpf, a, J, g) : adjoint_impl<double>(c, c->epd, c->bpd, a, J, g);
+}
+
+int mp_set_host_checkpoint_budget(mp_ctx *c, double bytes) {
+  if (!c) return MP_ERR_INVALID;
+  if (!(bytes >= 0) || !std::isfinite(bytes)) return set_err(c, MP_ERR_INVALID, "host checkpoint budget %g", bytes);
+  free_host_ckpt(c);
+  size_t S = 0;
+  for (const auto &r : state_regions(c)) S += r.second;
+  const long long n = S ? (long long)std::floor(bytes / double(S)) : 0;
+  // Each buffer: 2 MB-aligned memory marked for transparent huge pages, its
+  // pages faulted in by one thread per buffer (the host kernel zeroes them in
+  // parallel), then registered with the driver (fewer, larger pages to pin;
+  // cudaHostAlloc of 115 GB took 44-50 s).
+  const size_t align = size_t(2) << 20, len = (S + align - 1) / align * align;
+  std::vector<void *> bufs(size_t(n), nullptr);
+  std::vector<std::thread> th;
+  for (long long k = 0; k < n; ++k)
+    th.emplace_back([&, k] {
+      void *p = std::aligned_alloc(align, len);
+      if (!p) return;
+      madvise(p, len, MADV_HUGEPAGE);
+      std::memset(p, 0, len);
+      bufs[size_t(k)] = p;
+    });
+  for (auto &t : th) t.join();
+  long long k = 0;
+  cudaError_t e = cudaSuccess;
+  for (; k < n && bufs[size_t(k)]; ++k)
+    if ((e = cudaHostRegister(bufs[size_t(k)], len, cudaHostRegisterDefault)) != cudaSuccess) break;
+  if (k < n) {
+    cudaGetLastError();
+    for (long long q = 0; q < n; ++q) {
+      if (q < k) cudaHostUnregister(bufs[size_t(q)]);
+      std::free(bufs[size_t(q)]);
+    }
+    return set_err(c, MP_ERR_NO_MEMORY, "pinned host memory for checkpoint %lld of %lld (%zu B each): %s", k, n, S,
+                   e != cudaSuccess ? cudaGetErrorString(e) : "allocation failed");
+  }
+  c->host_ckpt = bufs;
+  return MP_OK;
 }
 
 }  // extern "C"

@@ -25,7 +25,7 @@ EXPORTED = (
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
-    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_state_size", "mp_save_state",
+    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_set_host_checkpoint_budget", "mp_state_size", "mp_save_state",
     "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max", "mp_kerr_counts",
     "mp_diag_file_name", "mp_hdf5_create", "mp_hdf5_write_field", "mp_hdf5_write_grid", "mp_hdf5_close",
 )
@@ -90,6 +90,8 @@ def lib():
     L.mp_objective.restype = C.c_int
     L.mp_adjoint.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp, dp, dp, dp]
     L.mp_adjoint.restype = C.c_int
+    L.mp_set_host_checkpoint_budget.argtypes = [vp, C.c_double]
+    L.mp_set_host_checkpoint_budget.restype = C.c_int
     L.mp_state_size.argtypes = [vp, C.POINTER(sz)]
     L.mp_state_size.restype = C.c_int
     L.mp_save_state.argtypes = [vp, vp, sz]
@@ -313,6 +315,11 @@ class Simulation:
         J = C.c_double()
         self._check(lib().mp_objective(self._h, C.byref(adj), C.byref(J)))
         return J.value
+
+    def set_host_checkpoint_budget(self, nbytes: float):
+        """Pinned host memory mp_adjoint may use for checkpoints
+        (mp_set_host_checkpoint_budget)."""
+        self._check(lib().mp_set_host_checkpoint_budget(self._h, float(nbytes)))
 
     def adjoint(self, adj: abi.AdjointConfig) -> tuple[float, dict]:
         """J and its gradient with respect to the design maps (mp_adjoint):

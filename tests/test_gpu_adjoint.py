@@ -133,6 +133,42 @@ def test_adjoint_memory_budget_schedule(per_cell):
         assert rel_l2(g1[name], g0[name]) <= 1e-13
 
 
+@pytest.mark.parametrize("steps", [30, 47])
+def test_adjoint_host_checkpoints(steps):
+    """A device budget of one state slot (every chunk run again from the start)
+    with room for segment checkpoints in host memory: the two-level schedule
+    runs fewer kernels and gives the same J and gradient as the whole history
+    (the recomputed forward steps are the same arithmetic)."""
+    cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
+    des = design_maps(cfg, 22)
+    init = clean_init(cfg, 23, smooth=True, scale=0.2)
+    full = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], steps)
+    with gpu_sim(cfg, init, des) as g:
+        J0, g0 = g.adjoint(full)
+    tight = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], steps,
+                               mem_budget=516 * cfg.field_count())
+    launches = {}
+    for nstates in (0, 12):
+        with gpu_sim(cfg, init, des) as g:
+            g.set_host_checkpoint_budget(nstates * len(g.save_state()))  # a saved state: one state and a header
+            l0 = g.launches
+            J1, g1 = g.adjoint(tight)
+            launches[nstates] = g.launches - l0
+            assert g.time == steps
+        assert abs(J1 - J0) <= 1e-14 * abs(J0)
+        for name in abi.DESIGN_NAMES[:2]:
+            assert rel_l2(g1[name], g0[name]) <= 1e-13
+    assert launches[12] < launches[0], launches
+
+
+def test_host_checkpoint_budget_rejects_bad_values():
+    cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
+    with gpu_sim(cfg, {}, {}) as g:
+        for bad in (-1.0, float("nan"), float("inf")):
+            with pytest.raises(runtime.MPulseError):
+                g.set_host_checkpoint_budget(bad)
+
+
 def test_adjoint_memory_budget_too_small():
     cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
     with gpu_sim(cfg, {}, {}) as g:

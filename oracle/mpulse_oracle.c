@@ -1464,6 +1464,31 @@ void mpo_faddeeva(const double *re, const double *im, double *wre, double *wim, 
 
 /* The incident field a source injects, for tests of the source kernels:
  * which = 0 -> getHField (E current), 1 -> getEField (H current). */
+/* The short-pulse closed forms at one point, for the reference's own table of
+ * them (test/testshortpulse.cpp: ShortPulseInjectSourceFunc::setParam(length,
+ * width, om0, Shift = 0, Phase, amp, eps), then Efunc and Bfunc at (x, y, z, t),
+ * printed without the amplitude): out = Re, Im of Efunc, Bfunc(bx = true),
+ * Bfunc(bx = false). */
+void mpo_short_pulse(double length, double width, double om0, double phase, double eps, double x, double y,
+                     double z, double t, double out[6]) {
+  oracle_faddeeva_init();
+  src_state st;
+  memset(&st, 0, sizeof st);
+  mp_source p;
+  memset(&p, 0, sizeof p);
+  p.length = length;
+  p.om0 = om0;
+  st.lightspeed = sqrt(1 / eps);
+  st.ZRl = 0.5 * om0 * width * width / st.lightspeed;
+  st.phase = 2 * M_PI * phase;
+  const double complex e = sp_efunc(&st, &p, x, y, z, t);
+  const double complex bx = sp_bfunc(&st, &p, x, y, z, t, 1);
+  const double complex by = sp_bfunc(&st, &p, x, y, z, t, 0);
+  out[0] = creal(e); out[1] = cimag(e);
+  out[2] = creal(bx); out[3] = cimag(bx);
+  out[4] = creal(by); out[5] = cimag(by);
+}
+
 int mpo_source_field(mpo_sim *s, int src, int which, int i, int j, int l, long long time, double out[3]) {
   if (src < 0 || src >= s->cfg.n_sources) return MP_ERR_INVALID;
   if (s->cfg.sources[src].kind == MP_SOURCE_GAUSS_BEAM) gauss_set_time(&s->src[src].gs[which ? 1 : 0], time);

@@ -47,6 +47,8 @@ def lib():
         L.mpo_set_time.restype = None
         L.mpo_faddeeva.argtypes = [C.POINTER(C.c_double)] * 4 + [C.c_size_t]
         L.mpo_faddeeva.restype = None
+        L.mpo_short_pulse.argtypes = [C.c_double] * 9 + [C.POINTER(C.c_double)]
+        L.mpo_short_pulse.restype = None
         L.mpo_source_field.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_longlong, C.POINTER(C.c_double)]
         L.mpo_source_field.restype = C.c_int
@@ -184,6 +186,14 @@ class OracleSim:
         if rc != abi.MP_OK:
             raise ValueError("mpo_source_field")
         return out
+
+
+def short_pulse(length, width, om0, phase, eps, x, y, z, t) -> np.ndarray:
+    """Re and Im of Efunc, Bfunc(bx) and Bfunc(by) of the short-pulse closed
+    form at one point (mpo_short_pulse)."""
+    out = (C.c_double * 6)()
+    lib().mpo_short_pulse(length, width, om0, phase, eps, x, y, z, t, out)
+    return np.array(out[:])
 
 
 def faddeeva(z: np.ndarray) -> np.ndarray:

@@ -149,6 +149,15 @@ struct mp_ctx {
   bool tma = false;    // TMA-staged kernels in use
   bool fused = false;  // the fused step kernel and its border kernel in use
   std::vector<void *> host_ckpt;  // pinned host buffers of one state each (mp_set_host_checkpoint_budget)
+  // CUDA graphs of K steps whose injection planes start at `planes` (small
+  // grids, where the launch gaps between the short half-step kernels cost)
+  struct StepGraph {
+    const void *planes;
+    int K;
+    cudaGraphExec_t exec;
+  };
+  std::vector<StepGraph> graphs;
+  bool use_graphs = false;
   ETmaMaps etma;
   BTmaMaps btma;
   // design region (mp_config.design_box): FP64 maps eps, Delta-eps factor, chi factor
@@ -800,6 +809,9 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
   // (E 1.12 ms, B 0.61 ms), whose 12 small tile copies per plane and block
   // serialise in the copy engine.
   c->fused = g.staging == MP_STAGING_FUSED;
+  // CUDA graphs for grids of up to 4 M cells, whose half steps take a few
+  // microseconds, so that the gaps between launches matter
+  c->use_graphs = (long long)g.nx * g.ny * g.nz <= (4LL << 20);
   if (g.staging == MP_STAGING_TMA) {
     if (!setup_tma(c)) return fail(set_err(c, MP_ERR_UNSUPPORTED, "TMA tensor maps could not be encoded"));
     // TMA kernels: two resident blocks per SM; about four waves of blocks so
@@ -949,6 +961,71 @@ int sources_ahead(mp_ctx *c, int want, const T **planes, int *steps) {
 // Process::time only), and each half step reads its step's plane pair.
 // Without gauss_inject and the per-kernel timer the next block is computed on
 // a second stream while the current one is stepped (sources_ahead).
+// The launches of K steps whose injection planes start at `planes` (plane q
+// of the batch at planes + 4 q plane).
+template <typename T>
+cudaError_t launch_steps(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const T *planes, int K) {
+  const size_t pl = size_t(c->plane);
+  for (int q = 0; q < K; ++q) {
+    if (c->nsrc) {
+      const T *base = planes + size_t(q) * 4 * pl;
+      ep.src[0].v0 = base;
+      ep.src[0].v1 = base + pl;
+      bp.src[0].v0 = base + 2 * pl;
+      bp.src[0].v1 = base + 3 * pl;
+    }
+    cudaError_t e = c->fused ? launch_step_fused<T>(ep, bp, c->mode, c->np, 1, c->stream)
+                    : c->tma ? launch_e_half_tma<T>(ep, c->etma, c->mode, c->np, c->stream)
+                             : launch_e_half<T>(ep, c->mode, c->np, c->stream);
+    if (e != cudaSuccess) return e;
+    e = c->fused ? launch_step_fused<T>(ep, bp, c->mode, c->np, 2, c->stream)
+        : c->tma ? launch_b_half_tma<T>(bp, c->btma, c->stream)
+                 : launch_b_half<T>(bp, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// The graph of K steps from `planes`, captured on first use (the kernels'
+// parameters are fixed for the context but for the injection planes; the
+// plane buffers are read when the graph runs).  *exec = nullptr when the
+// stream is being captured by the caller (the steps are then launched one by
+// one, into the caller's graph).
+template <typename T>
+int step_graph(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const T *planes, int K, cudaGraphExec_t *exec) {
+  *exec = nullptr;
+  cudaStreamCaptureStatus cs;
+  cudaError_t e = cudaStreamIsCapturing(c->stream, &cs);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamIsCapturing");
+  if (cs != cudaStreamCaptureStatusNone) return MP_OK;
+  for (const auto &g : c->graphs)
+    if (g.planes == planes && g.K == K) {
+      *exec = g.exec;
+      return MP_OK;
+    }
+  if (c->graphs.size() >= 16) {  // keep the most recent ones
+    cudaGraphExecDestroy(c->graphs.front().exec);
+    c->graphs.erase(c->graphs.begin());
+  }
+  cudaGraph_t graph = nullptr;
+  if ((e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return cuda_err(c, e, "cudaStreamBeginCapture");
+  const cudaError_t le = launch_steps<T>(c, ep, bp, planes, K);
+  e = cudaStreamEndCapture(c->stream, &graph);
+  if (le != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return cuda_err(c, le, "step kernels (graph capture)");
+  }
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamEndCapture");
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
+  c->graphs.push_back({planes, K, x});
+  *exec = x;
+  return MP_OK;
+}
+
 template <typename T>
 int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer *tm = nullptr,
               double *acc = nullptr, const StepHooks *hooks = nullptr) {
@@ -994,6 +1071,21 @@ int step_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, int n_steps, StepTimer 
         float ms;
         cudaEventElapsedTime(&ms, tm->ev[4], tm->ev[5]);
         acc[2] += ms;  // sources, all steps of the block
+      }
+    }
+    if (c->use_graphs && !tm && !hooks) {
+      // the batch as one CUDA graph (at most 64 steps per graph)
+      const int Kg = std::min(K, 64);
+      cudaGraphExec_t g;
+      const int rc = step_graph<T>(c, ep, bp, planes, Kg, &g);
+      if (rc != MP_OK) return rc;
+      if (g) {
+        NvtxRange nv("mp steps (graph)");
+        if ((e = cudaGraphLaunch(g, c->stream)) != cudaSuccess) return cuda_err(c, e, "cudaGraphLaunch");
+        c->launches += 2 * Kg;
+        c->time += Kg;
+        t += Kg;
+        continue;
       }
     }
     for (int q = 0; q < K; ++q) {
@@ -1152,6 +1244,7 @@ void mp_destroy(mp_ctx *c) {
   if (c->h_kerr) cudaFreeHost(c->h_kerr);
   if (c->h_diag) cudaFreeHost(c->h_diag);
   free_host_ckpt(c);
+  for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

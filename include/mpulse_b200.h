@@ -450,6 +450,14 @@ int mp_hdf5_write_field(mp_hdf5 *file, mp_ctx *ctx, const char *name);
  * order (dims[2] fastest), as the next dataset (what mp_hdf5_write_field
  * writes after assembling the grid). */
 int mp_hdf5_write_grid(mp_hdf5 *file, const double *data, const size_t dims[3]);
+/* FieldSliceDiag::write (src/fielddiag.cpp:56-115, "slicediag" with keys
+ * field, plane, pos): the plane of field `name` through MPulse index `pos`
+ * along axis `normal` (0: plane "x", 1: "y", 2: "z") over the full index
+ * range, as the next dataset of rank 2 with the dims reversed: for normal x
+ * the element of (j, k) is dataset[k][j], for y (i, k) -> [k][i], for z
+ * (i, j) -> [j][i].  Like MPulse, nothing is written when pos is not strictly
+ * inside the range (0 < pos < n + 1).  Synchronises ctx's stream. */
+int mp_hdf5_write_slice(mp_hdf5 *file, mp_ctx *ctx, const char *name, int normal, int pos);
 int mp_hdf5_close(mp_hdf5 *file);
 
 /* Checkpoint / restart of the whole device state: the six fields, the PLRC

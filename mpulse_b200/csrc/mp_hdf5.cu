@@ -1,6 +1,7 @@
 // mp_hdf5.cu - HDF5 field dumps of the device state, the output of MPulse's
-// FieldDiag (fielddiag.cpp:17-24, diagnostic.t:1-30) through HDFostream
-// (hdfstream.cpp:189-212, hdfstream.t:87-187).
+// FieldDiag (fielddiag.cpp:17-24, diagnostic.t:1-30) and FieldSliceDiag
+// (fielddiag.cpp:46-115) through HDFostream (hdfstream.cpp:189-212,
+// hdfstream.t:87-187).
 //
 // HDF5 is not a dependency of this library: the file is written by the small
 // encoder below, which emits the subset of the HDF5 file format (version 0
@@ -14,6 +15,7 @@
 //   - a grid of MPulse's full index range (ghost cells included) with index
 //     (i, j, k) has the dataspace {nz+2, ny+2, nx+2}, the dims reversed
 //     (hdfstream.t:110), i.e. the element of (i, j, k) is dataset[k][j][i];
+//     a slice is a rank-2 grid the same way (dataset[i2][i1]);
 //   - the file name is the pattern after DiagnosticInterface::parsedFileName
 //     (diagnostic.cpp:52-70): the first "#p" becomes the process id, the
 //     first "#t" the time step.
@@ -42,6 +44,7 @@ const int kMaxDatasets = 2 * kLeafK * 2 * kInternalK;  // one B-tree node of ful
 
 struct Dataset {
   std::string name;
+  int rank = 3;
   uint64_t dims[3];
   uint64_t data_addr, data_size;
   uint64_t header_addr = 0, name_off = 0;
@@ -109,11 +112,11 @@ Buf dataset_header(const Dataset &s) {
   Buf msgs;
   Buf sp;  // dataspace
   sp.u8(1);
-  sp.u8(3);
+  sp.u8(uint8_t(s.rank));
   sp.u8(0);  // no maximum dimensions
   sp.u8(0);
   sp.u32(0);
-  for (int q = 0; q < 3; ++q) sp.u64(s.dims[q]);
+  for (int q = 0; q < s.rank; ++q) sp.u64(s.dims[q]);
   message(msgs, 0x0001, sp);
   Buf ty;  // datatype: class 1 (floating point), version 1
   ty.u8(0x11);
@@ -181,14 +184,19 @@ int mp_hdf5_create(const char *pattern, int proc_id, long long time, mp_hdf5 **o
   return MP_OK;
 }
 
-int mp_hdf5_write_grid(mp_hdf5 *f, const double *data, const size_t dims[3]) {
-  if (!f || !data || !dims) return fail("mp_hdf5_write_grid: NULL argument");
-  if (int(f->sets.size()) >= kMaxDatasets) return fail("mp_hdf5_write_grid: at most 256 datasets per file");
+}  // extern "C"
+
+namespace {
+
+// The next dataset of the file: a rank-1..3 grid of doubles, C order.
+int write_dataset(mp_hdf5 *f, const double *data, int rank, const size_t *dims) {
+  if (int(f->sets.size()) >= kMaxDatasets) return fail("mp_hdf5: at most 256 datasets per file");
   Dataset s;
   const size_t n = f->sets.size();
   s.name = "data" + std::to_string(n);
+  s.rank = rank;
   size_t count = 1;
-  for (int q = 0; q < 3; ++q) {
+  for (int q = 0; q < rank; ++q) {
     s.dims[q] = uint64_t(dims[q]);
     count *= dims[q];
   }
@@ -201,15 +209,15 @@ int mp_hdf5_write_grid(mp_hdf5 *f, const double *data, const size_t dims[3]) {
     memcpy(&bits, &data[q], 8);
     for (int b = 0; b < 8; ++b) d.b[q * 8 + b] = (unsigned char)((bits >> (8 * b)) & 0xff);
   }
-  if (!write_at(f->fp, s.data_addr, d)) return fail("mp_hdf5_write_grid: write failed");
+  if (!write_at(f->fp, s.data_addr, d)) return fail("mp_hdf5: write failed");
   f->end += s.data_size;
   f->sets.push_back(s);
   return MP_OK;
 }
 
-int mp_hdf5_write_field(mp_hdf5 *f, mp_ctx *ctx, const char *field) {
-  if (!f || !ctx || !field) return fail("mp_hdf5_write_field: NULL argument");
-  if (int(f->sets.size()) >= kMaxDatasets) return fail("mp_hdf5_write_field: at most 256 datasets per file");
+// The field `field` of ctx over MPulse's full index range: (nx+2) (ny+2)
+// (nz+2) values, x fastest; x / y ghost cells are the periodic images.
+int full_grid(mp_ctx *ctx, const char *field, std::vector<double> &g, int dims[3]) {
   size_t count = 0;
   int rc = mp_field_size(ctx, field, &count);
   if (rc != MP_OK) return rc;
@@ -221,10 +229,9 @@ int mp_hdf5_write_field(mp_hdf5 *f, mp_ctx *ctx, const char *field) {
   int nx = 0, ny = 0, nz = 0;
   rc = mpb::ctx_grid(ctx, &nx, &ny, &nz);
   if (rc != MP_OK) return rc;
-  if (size_t(nz + 2) * ny * nx != count) return fail("mp_hdf5_write_field: not a full-grid field");
-  // MPulse's full range: x / y ghost cells are the periodic images
+  if (size_t(nz + 2) * ny * nx != count) return fail("mp_hdf5: not a full-grid field");
   const int NX = nx + 2, NY = ny + 2, NZ = nz + 2;
-  std::vector<double> g(size_t(NX) * NY * NZ);
+  g.assign(size_t(NX) * NY * NZ, 0.0);
   for (int k = 0; k < NZ; ++k)
     for (int j = 0; j < NY; ++j)
       for (int i = 0; i < NX; ++i) {
@@ -232,8 +239,52 @@ int mp_hdf5_write_field(mp_hdf5 *f, mp_ctx *ctx, const char *field) {
         const int jj = j == 0 ? ny : (j == ny + 1 ? 1 : j);
         g[(size_t(k) * NY + j) * NX + i] = plane[(size_t(k) * ny + (jj - 1)) * nx + (ii - 1)];
       }
-  const size_t dims[3] = {size_t(NZ), size_t(NY), size_t(NX)};
-  return mp_hdf5_write_grid(f, g.data(), dims);
+  dims[0] = NX;
+  dims[1] = NY;
+  dims[2] = NZ;
+  return MP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_hdf5_write_grid(mp_hdf5 *f, const double *data, const size_t dims[3]) {
+  if (!f || !data || !dims) return fail("mp_hdf5_write_grid: NULL argument");
+  return write_dataset(f, data, 3, dims);
+}
+
+int mp_hdf5_write_field(mp_hdf5 *f, mp_ctx *ctx, const char *field) {
+  if (!f || !ctx || !field) return fail("mp_hdf5_write_field: NULL argument");
+  if (int(f->sets.size()) >= kMaxDatasets) return fail("mp_hdf5_write_field: at most 256 datasets per file");
+  std::vector<double> g;
+  int n[3];
+  const int rc = full_grid(ctx, field, g, n);
+  if (rc != MP_OK) return rc;
+  const size_t dims[3] = {size_t(n[2]), size_t(n[1]), size_t(n[0])};
+  return write_dataset(f, g.data(), 3, dims);
+}
+
+int mp_hdf5_write_slice(mp_hdf5 *f, mp_ctx *ctx, const char *field, int normal, int pos) {
+  if (!f || !ctx || !field) return fail("mp_hdf5_write_slice: NULL argument");
+  if (normal < 0 || normal > 2) return fail("mp_hdf5_write_slice: normal must be 0 (x), 1 (y) or 2 (z)");
+  std::vector<double> g;
+  int n[3];
+  int rc = full_grid(ctx, field, g, n);
+  if (rc != MP_OK) return rc;
+  // FieldSliceDiag::fetchField: the slice is written only where pos lies
+  // strictly inside the index range (the stream is inactive otherwise)
+  if (!(pos > 0 && pos < n[normal] - 1)) return MP_OK;
+  if (int(f->sets.size()) >= kMaxDatasets) return fail("mp_hdf5_write_slice: at most 256 datasets per file");
+  const int d1 = normal == 0 ? 1 : 0, d2 = normal == 2 ? 1 : 2;
+  std::vector<double> sl(size_t(n[d1]) * n[d2]);
+  int i[3];
+  i[normal] = pos;
+  for (i[d2] = 0; i[d2] < n[d2]; ++i[d2])
+    for (i[d1] = 0; i[d1] < n[d1]; ++i[d1])
+      sl[size_t(i[d2]) * n[d1] + i[d1]] = g[(size_t(i[2]) * n[1] + i[1]) * n[0] + i[0]];
+  const size_t dims[2] = {size_t(n[d2]), size_t(n[d1])};
+  return write_dataset(f, sl.data(), 2, dims);
 }
 
 int mp_hdf5_close(mp_hdf5 *f) {
@@ -261,7 +312,9 @@ int mp_hdf5_close(mp_hdf5 *f) {
   for (const Dataset &s : sets) sorted.push_back(&s);
   std::sort(sorted.begin(), sorted.end(), [](const Dataset *a, const Dataset *b) { return a->name < b->name; });
   const int per = 2 * kLeafK;
-  const int nnodes = sorted.empty() ? 1 : int((sorted.size() + per - 1) / per);
+  // (a file with no dataset: a B-tree without entries, as HDF5 creates an
+  // empty group)
+  const int nnodes = int((sorted.size() + per - 1) / per);
   std::vector<uint64_t> snod_addr(nnodes), last_name(nnodes, 0);
   for (int q = 0; q < nnodes; ++q) {
     Buf sn;

@@ -27,7 +27,7 @@ EXPORTED = (
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
     "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_set_host_checkpoint_budget", "mp_state_size", "mp_save_state",
     "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max", "mp_kerr_counts",
-    "mp_diag_file_name", "mp_hdf5_create", "mp_hdf5_write_field", "mp_hdf5_write_grid", "mp_hdf5_close",
+    "mp_diag_file_name", "mp_hdf5_create", "mp_hdf5_write_field", "mp_hdf5_write_slice", "mp_hdf5_write_grid", "mp_hdf5_close",
 )
 
 _lib = None
@@ -112,6 +112,8 @@ def lib():
     L.mp_hdf5_create.restype = C.c_int
     L.mp_hdf5_write_field.argtypes = [vp, vp, cp]
     L.mp_hdf5_write_field.restype = C.c_int
+    L.mp_hdf5_write_slice.argtypes = [vp, vp, cp, C.c_int, C.c_int]
+    L.mp_hdf5_write_slice.restype = C.c_int
     L.mp_hdf5_write_grid.argtypes = [vp, dp, C.POINTER(sz)]
     L.mp_hdf5_write_grid.restype = C.c_int
     L.mp_hdf5_close.argtypes = [vp]
@@ -152,6 +154,14 @@ class Hdf5File:
     def write_field(self, sim: "Simulation", name: str):
         """FieldDiag::write: the field `name` of sim as the next dataset."""
         rc = lib().mp_hdf5_write_field(self._h, sim._h, name.encode())
+        if rc != abi.MP_OK:
+            raise MPulseError(rc, sim.last_error() or _global_error())
+
+    def write_slice(self, sim: "Simulation", name: str, plane: str, pos: int):
+        """FieldSliceDiag::write: the plane ("x", "y" or "z") of field `name`
+        through MPulse index pos as the next dataset (nothing when pos is not
+        strictly inside the grid)."""
+        rc = lib().mp_hdf5_write_slice(self._h, sim._h, name.encode(), "xyz".index(plane), int(pos))
         if rc != abi.MP_OK:
             raise MPulseError(rc, sim.last_error() or _global_error())
 

@@ -39,6 +39,14 @@ def test_host_arrays_round_trip(tmp_path, count):
         np.testing.assert_array_equal(got[want_names[q]], a)
 
 
+def test_file_without_datasets(tmp_path):
+    """An HDFostream that writes nothing (a slice on the boundary) leaves a
+    file whose root group has no entries."""
+    with runtime.Hdf5File(str(tmp_path / "empty.h5")) as f:
+        pass
+    assert read_datasets(f.name) == {}
+
+
 def test_too_many_datasets_is_an_error(tmp_path):
     arrays = [np.zeros((1, 1, 1))] * 257
     with pytest.raises(runtime.MPulseError) as e:
@@ -50,7 +58,7 @@ def _reference_records(path):
     """The datasets MPulse's HDFostream handed to the HDF5 stand-in for the
     file `path`: {name: array [k][j][i]} (the stand-in's grid is C order over
     (i, j, k); the dataspace MPulse declares is the reversed {nz+2, ny+2,
-    nx+2})."""
+    nx+2}; a slice likewise, rank 2)."""
     raw = open(path + ".raw", "rb").read()
     out = {}
     for line in open(path + ".calls"):
@@ -60,7 +68,7 @@ def _reference_records(path):
         dims = tuple(int(x) for x in parts[4:4 + rank])
         off, nbytes = int(parts[4 + rank]), int(parts[5 + rank])
         a = np.frombuffer(raw, dtype=np.float64, count=nbytes // 8, offset=off)
-        out[parts[1]] = a.reshape(dims[::-1]).transpose(2, 1, 0)
+        out[parts[1]] = a.reshape(dims[::-1]).T
         assert out[parts[1]].shape == dims
     return out
 
@@ -110,3 +118,57 @@ def test_dumps_match_mpulse_fielddiag(tmp_path, monkeypatch, case):
         for ds in want:
             assert got[ds].shape == want[ds].shape == (cfg.nz + 2, cfg.ny + 2, cfg.nx + 2)
             assert rel_l2(got[ds], want[ds]) <= 1e-12, (name, ds)
+
+
+@pytest.mark.gpu
+def test_slices_match_mpulse_slicediag(tmp_path, monkeypatch):
+    """MPulse's "slicediag" (FieldSliceDiag) writes a plane of a field per
+    output step: Ex in the plane y = 6 every 4 steps to "sy#t.h5", Bz in the
+    plane z = 3 every 3 steps appended to one file, and Ey at x = 0 (on the
+    boundary: an inactive stream, files without datasets).  The device state
+    written with mp_hdf5_write_slice at the same steps gives the same files,
+    dataset names, dims and values (FP64, <= 1e-12)."""
+    from oracle import pyoracle
+    from tests.cases import make_case, random_fields, rel_l2
+    if not os.path.exists(pyoracle.REF_BIN):
+        pytest.skip("reference build absent")
+    cfg = make_case("nonlin_all_short", abi.MP_FP64)
+    init = random_fields(cfg, seed=37)
+    steps = 9
+    ref_dir, our_dir = tmp_path / "ref", tmp_path / "ours"
+    ref_dir.mkdir()
+    our_dir.mkdir()
+    monkeypatch.setenv("MPULSE_REF_HDF5_LOG", "1")
+    diags = (f"slicediag {{ field Ex plane y pos 6 file {ref_dir}/sy#t.h5 interval 4 }} "
+             f"slicediag {{ field Bz plane z pos 3 file {ref_dir}/sz.h5 interval 3 append y }} "
+             f"slicediag {{ field Ey plane x pos 0 file {ref_dir}/sx#t.h5 interval 5 }}")
+    pyoracle.run_reference(cfg, steps, init, inits=diags, workdir=str(ref_dir))
+    with runtime.Simulation(cfg) as g:
+        for n, v in init.items():
+            g.upload(n, v)
+        appended = runtime.Hdf5File(f"{our_dir}/sz.h5", 0, 0)
+        for n in range(steps):
+            g.step(1)
+            if n % 4 == 0:
+                with runtime.Hdf5File(f"{our_dir}/sy#t.h5", 0, n) as f:
+                    f.write_slice(g, "Ex", "y", 6)
+            if n % 3 == 0:
+                appended.write_slice(g, "Bz", "z", 3)
+            if n % 5 == 0:
+                with runtime.Hdf5File(f"{our_dir}/sx#t.h5", 0, n) as f:
+                    f.write_slice(g, "Ey", "x", 0)
+        appended.close()
+    ref_files = sorted(p.name[:-len(".calls")] for p in ref_dir.glob("*.h5.calls"))
+    assert ref_files == ["sx0.h5", "sx5.h5", "sy0.h5", "sy4.h5", "sy8.h5", "sz.h5"]
+    assert sorted(p.name for p in our_dir.glob("*.h5")) == ref_files
+    shapes = {"sy": (cfg.nz + 2, cfg.nx + 2), "sz": (cfg.ny + 2, cfg.nx + 2)}
+    for name in ref_files:
+        want = _reference_records(str(ref_dir / name))
+        got = read_datasets(str(our_dir / name))
+        assert sorted(got) == sorted(want), name
+        if name.startswith("sx"):
+            assert not got
+        for ds in want:
+            assert got[ds].shape == want[ds].shape == shapes[name[:2]]
+            assert rel_l2(got[ds], want[ds]) <= 1e-12, (name, ds)
+    assert sorted(read_datasets(str(our_dir / "sz.h5"))) == ["data0", "data1", "data2"]

@@ -455,8 +455,10 @@ int mp_hdf5_write_grid(mp_hdf5 *file, const double *data, const size_t dims[3]);
  * along axis `normal` (0: plane "x", 1: "y", 2: "z") over the full index
  * range, as the next dataset of rank 2 with the dims reversed: for normal x
  * the element of (j, k) is dataset[k][j], for y (i, k) -> [k][i], for z
- * (i, j) -> [j][i].  Like MPulse, nothing is written when pos is not strictly
- * inside the range (0 < pos < n + 1).  Synchronises ctx's stream. */
+ * (i, j) -> [j][i].  Nothing is written when pos is not strictly inside the
+ * range (0 < pos < n + 1); MPulse's stream is then inactive and does not even
+ * create the file, so a caller following slicediag skips mp_hdf5_create for
+ * such a plane.  Synchronises ctx's stream. */
 int mp_hdf5_write_slice(mp_hdf5 *file, mp_ctx *ctx, const char *name, int normal, int pos);
 int mp_hdf5_close(mp_hdf5 *file);
 

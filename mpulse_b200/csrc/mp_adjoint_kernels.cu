@@ -175,7 +175,13 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
             bz_ym = ldg_c(Bz, base + colym, nf, st), bz_xm = ldg_c(Bz, base + colxm, nf, st);
     const R kzk = p.ikH[2][k], kzm = p.ikH[2][k - 1];
     R a[3] = {R(ld_c(p.Eb[0], c0, nf, st)), R(ld_c(p.Eb[1], c0, nf, st)), R(ld_c(p.Eb[2], c0, nf, st))};
-    const R En[3] = {R(ldg_c(p.En[0], c0, nf, st)), R(ldg_c(p.En[1], c0, nf, st)), R(ldg_c(p.En[2], c0, nf, st))};
+    // E^n enters here only through the Kerr term (its coefficient is zero in
+    // a linear medium) and the |E|^2 objective's box: elsewhere it is not read
+    R En[3] = {R(0), R(0), R(0)};
+    if (plrc_nl || (p.add_obj && oxy && p.obj_kind == 1 && k >= p.oz0 && k <= p.oz1)) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) En[c] = R(ldg_c(p.En[c], c0, nf, st));
+    }
     R En1[3] = {R(0), R(0), R(0)};
     if (med && (plrc_nl || dcell)) {
 #pragma unroll

@@ -709,9 +709,15 @@ int create_impl(const mp_config *cfg, mp_ctx **out) {
         ShortPulse sp;
         sp.c = p.lightspeed; sp.ZRl = p.ZRl; sp.phase = 0.0; sp.T = q.length; sp.om0 = q.om0;
         sp.coef = wcoef.data(); sp.L = wL;
+        short_pulse_constants(sp);
         const double Exmax = short_pulse_e(sp, 0, 0, 0, 0).re;
         p.amp = q.amp / Exmax;
         p.phase = 2 * M_PI * q.phase;
+        sp.phase = p.phase;
+        short_pulse_constants(sp);
+        p.sp_eiphi[0] = sp.eiphi.re; p.sp_eiphi[1] = sp.eiphi.im;
+        p.sp_emip[0] = sp.emip.re; p.sp_emip[1] = sp.emip.im;
+        p.sp_g = sp.g;
         p.tshift = q.t_shift;
         p.zshift = q.z_shift;
         p.w_coef = c->d_wcoef;

@@ -232,6 +232,7 @@ struct SourceEvalParams {
   double k[3], amp3[3], bg[3], om, ramp, width, offset;
   // short pulse
   double lightspeed, ZRl, amp, phase, tshift, zshift, length, om0;
+  double sp_eiphi[2], sp_emip[2], sp_g;  // exp(2 i phase), exp(-i phase), exp(-(om0 length / 2)^2)
   double centre[3];
   const double *w_coef;   // Faddeeva expansion coefficients (highest power first)
   double w_L;

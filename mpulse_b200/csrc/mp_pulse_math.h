@@ -100,25 +100,37 @@ struct ShortPulse {
   double c, ZRl, phase, T, om0;
   const double *coef;
   double L;
+  // constants of the pulse, set by short_pulse_constants: exp(2 i phase),
+  // exp(-i phase), exp(-tb^2) with tb = om0 T / 2
+  cd eiphi, emip;
+  double g;
 };
+
+// The pulse's constants (once per source, not per point).
+MPB_HD void short_pulse_constants(ShortPulse &sp) {
+  const double tb = 0.5 * sp.om0 * sp.T;
+  sp.eiphi = cexp_(cd(0.0, 2.0 * sp.phase));
+  sp.emip = cexp_(cd(0.0, -sp.phase));
+  sp.g = exp(-tb * tb);
+}
 
 // Efunc (shortpulsefunctions.cpp:28-94).
 MPB_HD cd short_pulse_e(const ShortPulse &sp, double x, double y, double z, double t) {
   const cd I = I_();
-  const double c = sp.c, p = sp.phase, T = sp.T, T2 = T * T, T4 = T2 * T2;
+  const double c = sp.c, T = sp.T, T2 = T * T, T4 = T2 * T2;
   const double tb = 0.5 * sp.om0 * T;
   const double r2 = x * x + y * y;
   const cd q(z, sp.ZRl);
   const cd rT = sp.ZRl / q;
   const cd rpiT = sqrt(M_PI) * rT;
   const cd rpT = -sp.ZRl / (q * q);
-  const cd eiphi = cexp_(2.0 * I * p);
+  const cd eiphi = sp.eiphi;
   const cd tpT = (t - z / c) - r2 / (2. * c * q);
   const cd tpT2 = tpT * tpT;
   const cd tpzT = (-1 / c) - r2 / (2. * c * q * q);
   cd an = -I * tb + tpT / T;
   cd ap = I * tb + tpT / T;
-  const cd A = cexp_(-I * p) / (rpiT * T4);
+  const cd A = sp.emip / (rpiT * T4);
   const cd B = rT * T * (I * (1.0 + eiphi) * rpT * T2 -
                          rT * (T * (-I - 2 * tb + eiphi * (-I + 2 * tb)) + 2.0 * I * (1.0 + eiphi) * tpT) * tpzT);
   cd C = I * eiphi * rpiT * (T * tb + I * tpT) * (rpT * T2 + 2.0 * I * rT * T * tb * tpzT - 2.0 * rT * tpT * tpzT);
@@ -134,7 +146,7 @@ MPB_HD cd short_pulse_e(const ShortPulse &sp, double x, double y, double z, doub
     ap = -ap;
     D = -D;
   }
-  const cd Ef = S + A * exp(-tb * tb) * (B + C * faddeeva(an, sp.coef, sp.L) - D * faddeeva(ap, sp.coef, sp.L));
+  const cd Ef = S + A * sp.g * (B + C * faddeeva(an, sp.coef, sp.L) - D * faddeeva(ap, sp.coef, sp.L));
   return -I * Ef;
 }
 
@@ -142,7 +154,7 @@ MPB_HD cd short_pulse_e(const ShortPulse &sp, double x, double y, double z, doub
 // by -> i (D-terms - B-terms).
 MPB_HD cd short_pulse_b(const ShortPulse &sp, double x, double y, double z, double t, bool bx) {
   const cd I = I_();
-  const double c = sp.c, p = sp.phase, T = sp.T, T2 = T * T, T4 = T2 * T2;
+  const double c = sp.c, T = sp.T, T2 = T * T, T4 = T2 * T2;
   const double tb = 0.5 * sp.om0 * T;
   const double r2 = x * x + y * y;
   const cd q(z, sp.ZRl);
@@ -152,7 +164,7 @@ MPB_HD cd short_pulse_b(const ShortPulse &sp, double x, double y, double z, doub
   const cd rpiT = sqrt(M_PI) * rT;
   const cd rpT = -sp.ZRl / (q * q);
   const cd rppT = 2. * sp.ZRl / (q * q * q);
-  const cd eiphi = cexp_(2.0 * I * p);
+  const cd eiphi = sp.eiphi;
   const cd tpT = (t - z / c) - r2 / (2. * c * q);
   const cd tpT2 = tpT * tpT;
   const cd tpzT = (-1 / c) + r2 / (2. * c * q * q);
@@ -169,8 +181,8 @@ MPB_HD cd short_pulse_b(const ShortPulse &sp, double x, double y, double z, doub
   cd an = -I * tb + tpT / T;
   cd ap = I * tb + tpT / T;
   const cd common = T * (-I - 2 * tb + eiphi * (-I + 2 * tb)) + 2.0 * I * (1.0 + eiphi) * tpT;
-  const cd eA = cexp_(-I * p) / (sqrt(M_PI) * T4);
-  const double g = exp(-tb * tb);
+  const cd eA = sp.emip / (sqrt(M_PI) * T4);
+  const double g = sp.g;
   cd e1(0.0), e2(0.0);
   const bool neg_n = an.im < 0, neg_p = ap.im < 0;
   if (neg_n) { e1 = cexp_(2.0 * I * tpT * tb / T - tpT2 / T2); an = -an; }
@@ -190,7 +202,7 @@ MPB_HD cd short_pulse_b(const ShortPulse &sp, double x, double y, double z, doub
   cd BC = -tpxT2 * 2.0 * eiphi * rpiT * aip2 + I * T2 * tpxxT * eiphi * rpiT * aip;
   cd BD = -tpxT2 * 2.0 * rpiT * ain2 + I * T2 * tpxxT * rpiT * (-(T * tb) + I * tpT);
   cd BS(0.0);
-  const cd eD = cexp_(-I * p) / (2. * sqrt(M_PI) * T4);
+  const cd eD = sp.emip / (2. * sqrt(M_PI) * T4);
   const cd DB = 2.0 * T * (2.0 * I * (1.0 + eiphi) * rpT * T2 * tpzT -
                            rT * (T * (-I - 2 * tb + eiphi * (-I + 2 * tb)) * tpzT2 +
                                  I * (1.0 + eiphi) * (2.0 * tpT * tpzT2 - T2 * tpzzT)));

@@ -49,6 +49,9 @@ __device__ void short_pulse_field(const SourceEvalParams &q, int i, int j, int l
   ShortPulse sp;
   sp.c = q.lightspeed; sp.ZRl = q.ZRl; sp.phase = q.phase; sp.T = q.length; sp.om0 = q.om0;
   sp.coef = q.w_coef; sp.L = q.w_L;
+  sp.eiphi = cd(q.sp_eiphi[0], q.sp_eiphi[1]);
+  sp.emip = cd(q.sp_emip[0], q.sp_emip[1]);
+  sp.g = q.sp_g;
   out[2] = 0.0;
   if (q.isH) {
     const double posxh = (i + 0.5 - q.centre[0]) * q.dx;

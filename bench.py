@@ -490,10 +490,11 @@ def run_other_configs(local_rank: int, torch, stream) -> dict:
 def run_adjoint(local_rank: int) -> dict:
     """The adjoint workload (96^3, single-pole medium, 32^3 design region,
     1500 steps, |E|^2 monitor objective): wall time of the forward run that
-    computes J (mp_objective) and of mp_adjoint (forward with checkpoints +
-    reverse pass), best of three; FP32 with a checkpoint every 50 steps (the
-    workload's schedule) and with the whole E history kept, and the FP32
-    gradient against the FP64 one."""
+    computes J (mp_objective), of mp_adjoint (forward with checkpoints +
+    reverse pass) and of the same in two calls (mp_objective_record, then
+    mp_adjoint_reverse), best of three; FP32 and FP64 with a checkpoint every
+    50 steps (the workload's schedule) and with the whole E history kept, and
+    the FP32 gradient against the FP64 one."""
     from mpulse_b200 import runtime
 
     out = {"workload": "adjoint_plrc_96^3_design32^3_1500steps", "unit": "s"}
@@ -526,10 +527,27 @@ def run_adjoint(local_rank: int) -> dict:
         fwd, J = timed(lambda g: g.objective(adj))
         t_adj, (Ja, gr) = timed(lambda g: g.adjoint(adj))
         t_full, _ = timed(lambda g: g.adjoint(full))
+        # the same gradient in two calls: the forward run keeping the
+        # checkpoints (mp_objective_record), then the reverse pass
+        # (mp_adjoint_reverse), each timed on its own, best of three
+        t_rec = t_rev = None
+        for _ in range(3):
+            with fresh() as g:
+                t0 = time.perf_counter()
+                g.objective_record(adj)
+                t1 = time.perf_counter()
+                _, grr = g.adjoint_reverse()
+                t2 = time.perf_counter()
+            t_rec = t1 - t0 if t_rec is None else min(t_rec, t1 - t0)
+            t_rev = t2 - t1 if t_rev is None else min(t_rev, t2 - t1)
         grads[tag] = gr["DesignEps"]
         out[tag] = {"forward_s": round(fwd, 4), "adjoint_s": round(t_adj, 4),
                     "ratio": round(t_adj / fwd, 3), "checkpoint_every": adj.checkpoint_every,
                     "adjoint_full_history_s": round(t_full, 4), "ratio_full_history": round(t_full / fwd, 3),
+                    "record_s": round(t_rec, 4), "reverse_s": round(t_rev, 4),
+                    "ratio_reverse": round(t_rev / fwd, 3),
+                    "ratio_record_plus_reverse": round((t_rec + t_rev) / fwd, 3),
+                    "reverse_gradient_equals_adjoint": all(np.array_equal(grr[k], gr[k]) for k in gr),
                     "J": J}
     g32, g64 = grads["fp32"], grads["fp64"]
     out["grad_rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))

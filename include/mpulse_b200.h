@@ -490,6 +490,26 @@ int mp_objective(mp_ctx *ctx, const mp_adjoint_config *adj, double *J);
 int mp_adjoint(mp_ctx *ctx, const mp_adjoint_config *adj, double *J, double *grad_eps,
                double *grad_deps_scale, double *grad_chi_scale);
 
+/* mp_adjoint in two calls, as an autograd tape: mp_objective_record runs the
+ * forward part of mp_adjoint for adj (the steps, J in *J, and the checkpoints
+ * of mp_adjoint's schedule, with the E history of the last segment) and keeps
+ * them in the context: the device memory mp_adjoint would use, beside the
+ * state.  mp_adjoint_reverse then runs the rest (the reverse pass, recomputing
+ * the other segments from their checkpoints) and releases the record; J (may
+ * be NULL) and the gradients are those mp_adjoint gives for the same run, to
+ * the last bit, and the state ends as after mp_objective_record.  A record is
+ * released by mp_release_record, by the next mp_objective_record, and by
+ * every call that steps the context or writes its state, time, design maps,
+ * stream or host checkpoint buffers (mp_step, mp_step_async, mp_kernel_times,
+ * mp_upload, mp_set_time, mp_load_state, mp_initialize, mp_objective,
+ * mp_adjoint, mp_set_stream, mp_set_host_checkpoint_budget, mp_destroy);
+ * mp_adjoint_reverse without a record returns MP_ERR_INVALID.  Writes through
+ * mp_device_field pointers are not seen: the reverse pass reads only the
+ * record and the design maps.  No counterpart in MPulse. */
+int mp_objective_record(mp_ctx *ctx, const mp_adjoint_config *adj, double *J);
+int mp_adjoint_reverse(mp_ctx *ctx, double *J, double *grad_eps, double *grad_deps_scale, double *grad_chi_scale);
+int mp_release_record(mp_ctx *ctx);
+
 /* Reserves pinned host memory for mp_adjoint's checkpoints: as many buffers
  * of one forward state each as fit in `bytes` (allocated and pinned now, which
  * takes seconds for tens of GB; freed by the next call or mp_destroy; 0 frees

@@ -25,6 +25,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <new>
 #include <string>
 #include <thread>
@@ -93,6 +94,8 @@ struct LayerHost {
 
 }  // namespace
 
+struct AdjRecord;
+
 struct mp_ctx {
   mp_config cfg;
   int fp32 = 0;
@@ -149,6 +152,7 @@ struct mp_ctx {
   bool tma = false;    // TMA-staged kernels in use
   bool fused = false;  // the fused step kernel and its border kernel in use
   std::vector<void *> host_ckpt;  // pinned host buffers of one state each (mp_set_host_checkpoint_budget)
+  AdjRecord *rec = nullptr;       // the run mp_objective_record kept for mp_adjoint_reverse
   // CUDA graphs of K steps whose injection planes start at `planes` (small
   // grids, where the launch gaps between the short half-step kernels cost)
   struct StepGraph {
@@ -1228,9 +1232,15 @@ static void free_host_ckpt(mp_ctx *c) {
   c->host_ckpt.clear();
 }
 
+// Frees what mp_objective_record kept (defined with the adjoint below).  Every
+// call that steps the context or writes its state, time, design maps, stream or
+// host checkpoint buffers releases it first.
+static void release_record(mp_ctx *c);
+
 void mp_destroy(mp_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->src_stream) {
     cudaStreamSynchronize(c->src_stream);
@@ -1257,6 +1267,7 @@ void mp_destroy(mp_ctx *c) {
 
 int mp_set_stream(mp_ctx *c, void *s) {
   if (!c) return MP_ERR_INVALID;
+  release_record(c);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamSynchronize");
   c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
@@ -1278,6 +1289,7 @@ int mp_field_size(mp_ctx *c, const char *name, size_t *count) {
 
 int mp_upload(mp_ctx *c, const char *name, const double *host, size_t count) {
   if (!c || !host) return MP_ERR_INVALID;
+  release_record(c);
   const int dm = design_map(c, name);
   if (dm >= 0) {
     if (count != c->dcells) return set_err(c, MP_ERR_INVALID, "%s: %zu values, expected %zu", name, count, c->dcells);
@@ -1360,6 +1372,7 @@ int mp_download(mp_ctx *c, const char *name, double *host, size_t count) {
 int mp_step_async(mp_ctx *c, int n_steps) {
   if (!c || n_steps < 0) return MP_ERR_INVALID;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   return c->fp32 ? step_impl<float>(c, c->epf, c->bpf, n_steps) : step_impl<double>(c, c->epd, c->bpd, n_steps);
 }
 
@@ -1400,6 +1413,7 @@ int mp_get_time(mp_ctx *c, long long *t) {
 
 int mp_set_time(mp_ctx *c, long long t) {
   if (!c) return MP_ERR_INVALID;
+  release_record(c);
   c->time = t;
   return MP_OK;
 }
@@ -1461,6 +1475,7 @@ int mp_field_energy(mp_ctx *c, double *energy) {
 int mp_kernel_times(mp_ctx *c, int n_steps, double *e_ms, double *b_ms, double *s_ms) {
   if (!c || n_steps < 1 || !e_ms || !b_ms || !s_ms) return MP_ERR_INVALID;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   StepTimer tm;
   for (int q = 0; q < 6; ++q) {
     cudaError_t e = cudaEventCreate(&tm.ev[q]);
@@ -1836,15 +1851,57 @@ bool plan_two_level(long long Tn, double budget, double host_budget, size_t S, s
   return found;
 }
 
+// Phases of adjoint_impl: the whole of mp_adjoint; the forward part alone
+// (mp_objective_record), which stops once the first run has reached the end;
+// the reverse part alone (mp_adjoint_reverse), from what the forward part kept.
+enum AdjPhase { kAdjAll = 0, kAdjRecord = 1, kAdjReverse = 2 };
+const int kAdjStop = 1 << 20;  // returned through revolve when the forward part is done
+
+}  // namespace
+
+// What mp_objective_record keeps for mp_adjoint_reverse: the objective, the
+// schedule, the checkpoint slots (the run's start and chunk starts, and its end
+// state), the history buffers (the last chunk's E history in buffer 0) and the
+// objective terms, in device memory freed with the record.
+struct AdjRecord {
+  DevBufs buf;
+  mp_adjoint_config a;
+  long long t0 = 0;  // the time the run started at
+  double J = 0;
+  long long Kh = 0;
+  int slots = 0, nbuf = 1;
+  bool two = false;
+  TwoLevel tl;
+  char *ckpt = nullptr, *hist[2] = {nullptr, nullptr};
+  double *terms = nullptr;
+  explicit AdjRecord(cudaStream_t s) : buf(s) {}
+};
+
+static void release_record(mp_ctx *c) {
+  if (!c->rec) return;
+  cudaSetDevice(c->cfg.device);
+  delete c->rec;  // waits for the stream, frees the buffers
+  c->rec = nullptr;
+}
+
+namespace {
+
 // The forward run and the reverse pass on the schedule of plan_schedule /
 // revolve: each chunk [n0, n1) is run forward from the live state or a
 // checkpoint keeping E (and, for the Sz objective, Bx and By on the plane) of
 // every state n0..n1, then stepped back with adj_e / adj_b from n1 - 1 down to
 // n0.  The last chunk is reversed straight after the first run reaches it, so
-// with one chunk nothing is recomputed.
+// with one chunk nothing is recomputed.  The reverse phase runs the same
+// schedule from the record and skips what the recorded run did (the saves, the
+// advances and the forward run of the last chunk), so both phases together do
+// what the whole does, in the same order.
 template <typename T>
-int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_config *a, double *J, double *gout[3]) {
+int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_config *a, double *J, double *gout[3],
+                 AdjPhase phase = kAdjAll) {
   const mp_config &g = c->cfg;
+  AdjRecord *rec = phase == kAdjReverse ? c->rec : nullptr;
+  if (phase == kAdjReverse && !rec) return set_err(c, MP_ERR_INVALID, "no recorded run");
+  if (rec) a = &rec->a;
   const long long Tn = a->steps;
   const auto regions = state_regions(c);
   size_t S = 0;
@@ -1855,34 +1912,52 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   long long Kh = 0;  // steps per history chunk
   int slots = 0;     // state checkpoints (the initial state included)
   int nbuf = 1;      // history buffers
-  if (!plan_schedule(Tn, a->checkpoint_every, a->mem_budget, S, H, &Kh, &slots, &nbuf))
-    return set_err(c, MP_ERR_NO_MEMORY,
-                   "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
-                   a->mem_budget, S, H);
-  // segments whose starts go to host memory, under a budget (not with an
-  // explicit checkpoint_every)
-  TwoLevel tl;
-  const bool two = a->checkpoint_every <= 0 && Kh < Tn &&
-                   plan_two_level(Tn, a->mem_budget, double(c->host_ckpt.size()) * double(S), S, H,
-                                  schedule_steps(Tn, Kh, slots), &tl);
-  if (two) {
-    Kh = tl.Kh;
-    slots = tl.slots;
-    nbuf = tl.nbuf;
+  TwoLevel tl;       // segments whose starts go to host memory
+  bool two = false;
+  if (rec) {
+    Kh = rec->Kh;
+    slots = rec->slots;
+    nbuf = rec->nbuf;
+    two = rec->two;
+    tl = rec->tl;
+  } else {
+    if (!plan_schedule(Tn, a->checkpoint_every, a->mem_budget, S, H, &Kh, &slots, &nbuf))
+      return set_err(c, MP_ERR_NO_MEMORY,
+                     "mem_budget %.4g B holds no schedule (state %zu B per checkpoint, %zu B per step of history)",
+                     a->mem_budget, S, H);
+    // two levels only under a budget (not with an explicit checkpoint_every)
+    two = a->checkpoint_every <= 0 && Kh < Tn &&
+          plan_two_level(Tn, a->mem_budget, double(c->host_ckpt.size()) * double(S), S, H,
+                         schedule_steps(Tn, Kh, slots), &tl);
+    if (two) {
+      Kh = tl.Kh;
+      slots = tl.slots;
+      nbuf = tl.nbuf;
+    }
   }
   const long long K = Kh;
 
-  DevBufs buf(c->stream);
+  DevBufs buf(c->stream);  // the buffers of this call
+  // the forward part's buffers go to the record it makes
+  std::unique_ptr<AdjRecord> made(phase == kAdjRecord ? new AdjRecord(c->stream) : nullptr);
+  DevBufs &sbuf = made ? made->buf : buf;
   cudaError_t e;
   char *ckpt, *hist[2] = {nullptr, nullptr};
   double *terms;
-  if ((e = buf.alloc(reinterpret_cast<void **>(&ckpt), size_t(slots + 1) * S)) != cudaSuccess ||
-      (e = buf.alloc(reinterpret_cast<void **>(&hist[0]), size_t(K + 1) * H)) != cudaSuccess ||
-      (e = buf.alloc(reinterpret_cast<void **>(&terms), (size_t(Tn) + 1) * sizeof(double))) != cudaSuccess)
-    return cuda_err(c, e, "checkpoint allocation");
-  if (nbuf == 2 && buf.alloc(reinterpret_cast<void **>(&hist[1]), size_t(K + 1) * H) != cudaSuccess) {
-    cudaGetLastError();  // no room for the second buffer: chunks run forward and back in turn
-    nbuf = 1;
+  if (rec) {
+    ckpt = rec->ckpt;
+    hist[0] = rec->hist[0];
+    hist[1] = rec->hist[1];
+    terms = rec->terms;
+  } else {
+    if ((e = sbuf.alloc(reinterpret_cast<void **>(&ckpt), size_t(slots + 1) * S)) != cudaSuccess ||
+        (e = sbuf.alloc(reinterpret_cast<void **>(&hist[0]), size_t(K + 1) * H)) != cudaSuccess ||
+        (e = sbuf.alloc(reinterpret_cast<void **>(&terms), (size_t(Tn) + 1) * sizeof(double))) != cudaSuccess)
+      return cuda_err(c, e, "checkpoint allocation");
+    if (nbuf == 2 && sbuf.alloc(reinterpret_cast<void **>(&hist[1]), size_t(K + 1) * H) != cudaSuccess) {
+      cudaGetLastError();  // no room for the second buffer: chunks run forward and back in turn
+      nbuf = 1;
+    }
   }
   // The reverse pass runs on a second stream: the adjoint kernels of one chunk
   // overlap the forward run of the next, which only shares the history buffer
@@ -1910,7 +1985,7 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       return cuda_err(c, e, "cudaEventCreate");
   int cur = 0;  // history buffer of the chunk being run forward
   AdjParams<T> p = AdjParams<T>();
-  for (int q = 0; q < 3; ++q) {
+  for (int q = 0; q < 3 && phase != kAdjRecord; ++q) {
     void *eb, *bb, *gg;
     double *gr;
     if ((e = buf.alloc(&eb, fbytes)) != cudaSuccess || (e = buf.alloc(&bb, fbytes)) != cudaSuccess ||
@@ -1922,19 +1997,19 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     p.G[q] = static_cast<T *>(gg);
     p.grad[q] = gr;
   }
-  for (int s = 0; s < c->np; ++s)
+  for (int s = 0; s < c->np && phase != kAdjRecord; ++s)
     for (int q = 0; q < 3; ++q) {
       void *ps;
       if ((e = buf.alloc(&ps, 2 * c->psi_cells * sizeof(T))) != cudaSuccess) return cuda_err(c, e, "adjoint allocation");
       p.psib[s][q] = static_cast<T *>(ps);
     }
-  {
+  if (phase != kAdjRecord) {
     void *dp = nullptr;
     if (c->np > 0 && (e = buf.alloc(&dp, c->dcells * c->np * 6 * sizeof(T))) != cudaSuccess)
       return cuda_err(c, e, "adjoint allocation");
     p.dpsi = static_cast<T *>(dp);
   }
-  for (int isH = 0; isH < 2; ++isH) {
+  for (int isH = 0; isH < 2 && phase != kAdjRecord; ++isH) {
     const int rc = adj_faces<T>(c, buf, isH != 0, isH ? bp.cpml : ep.cpml, isH ? p.fh : p.fe);
     if (rc != MP_OK) return rc;
   }
@@ -2041,9 +2116,10 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     for (int q = 0; q < 3; ++q) ep.hist[q] = slot < 0 ? nullptr : const_cast<T *>(slot_e(slot, q));
   };
   // ---- forward and reverse on the checkpoint schedule
-  const long long t0 = c->time;
+  const long long t0 = rec ? rec->t0 : c->time;
   long long reached = 0;  // steps whose objective term is computed
   bool at_end = false;
+  bool skipping = rec != nullptr;  // replaying what the recorded run did
   // Forward steps n0..n1-1 from the live state in one batched call: the E
   // kernel of step n stores the new E into history slot n + 1 - h0 when
   // n >= h0 (h0 < 0: no history), the Sz planes are copied after it, and the
@@ -2069,34 +2145,51 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     return r;
   };
   RevolveOps ops;
-  ops.restore = [&](long long at, int slot) {
+  ops.restore = [&](long long at, int slot) -> int {
+    if (skipping) return MP_OK;
     const cudaError_t err = copy_state(slot, false);
     c->time = t0 + at;
     return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint restore");
   };
-  ops.save = [&](long long, int slot) {
+  ops.save = [&](long long, int slot) -> int {
+    if (skipping) return MP_OK;
     const cudaError_t err = copy_state(slot, true);
     return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint copy");
   };
-  ops.advance = [&](long long from, long long to) {
+  ops.advance = [&](long long from, long long to) -> int {
+    if (skipping) {
+      reached = std::max(reached, to);
+      return MP_OK;
+    }
     NvtxRange nv("mp_adjoint forward");
     return run(from, to, -1);
   };
   ops.leaf = [&](long long n0, long long n1) -> int {
     NvtxRange nv("mp_adjoint chunk");
     cudaError_t err;
-    // the buffer is free once the reverse pass of the chunk that used it is done
-    if (rs.used[cur] && (err = cudaStreamWaitEvent(c->stream, rs.rev[cur], 0)) != cudaSuccess)
-      return cuda_err(c, err, "cudaStreamWaitEvent");
-    if ((err = record(0, true)) != cudaSuccess) return cuda_err(c, err, "history copy");
-    int r = run(n0, n1, n0);
-    if (r != MP_OK) return r;
     const bool first = n1 == Tn && !at_end;
-    if (first) {
-      // the first time the run reaches the end: J, the final state
+    if (skipping) {
+      // the recorded run ended with this chunk's forward run: its history is
+      // in buffer 0, J and the final state are kept
+      if (!first || cur != 0) return set_err(c, MP_ERR_INVALID, "recorded schedule does not replay");
+      skipping = false;
       at_end = true;
-      if ((err = copy_state(slots, true)) != cudaSuccess) return cuda_err(c, err, "checkpoint copy");
-      if ((r = read_sum(c, terms, Tn, J)) != MP_OK || (r = mp_check_status(c)) != MP_OK) return r;
+      reached = Tn;
+      if (J) *J = rec->J;
+    } else {
+      // the buffer is free once the reverse pass of the chunk that used it is done
+      if (rs.used[cur] && (err = cudaStreamWaitEvent(c->stream, rs.rev[cur], 0)) != cudaSuccess)
+        return cuda_err(c, err, "cudaStreamWaitEvent");
+      if ((err = record(0, true)) != cudaSuccess) return cuda_err(c, err, "history copy");
+      int r = run(n0, n1, n0);
+      if (r != MP_OK) return r;
+      if (first) {
+        // the first time the run reaches the end: J, the final state
+        at_end = true;
+        if ((err = copy_state(slots, true)) != cudaSuccess) return cuda_err(c, err, "checkpoint copy");
+        if ((r = read_sum(c, terms, Tn, J)) != MP_OK || (r = mp_check_status(c)) != MP_OK) return r;
+        if (phase == kAdjRecord) return kAdjStop;
+      }
     }
     if ((err = cudaEventRecord(rs.fwd[cur], c->stream)) != cudaSuccess ||
         (err = cudaStreamWaitEvent(rs.s, rs.fwd[cur], 0)) != cudaSuccess)
@@ -2128,15 +2221,15 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     cur = (cur + 1) % nbuf;
     return MP_OK;
   };
-  int rc = MP_OK;
   long long live = 0;
-  if (!two) {
-    if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
-    std::vector<int> free_slots;
-    for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
-    rc = revolve(0, Tn, 0, free_slots, K, ops, live);
-    if (rc != MP_OK) return rc;
-  } else {
+  // the whole schedule, on one level or two (kAdjStop: the forward part is done)
+  auto run_schedule = [&]() -> int {
+    if (!two) {
+      if (!skipping && (e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+      std::vector<int> free_slots;
+      for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
+      return revolve(0, Tn, 0, free_slots, K, ops, live);
+    }
     // the live state to / from the host copy of segment k, on the stream
     auto host_copy = [&](long long k, bool save) -> cudaError_t {
       size_t off = 0;
@@ -2149,10 +2242,11 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
       }
       return cudaSuccess;
     };
+    int r;
     // first run: the start of every segment to host memory
     for (long long k = 0; k < tl.nseg; ++k) {
-      if ((e = host_copy(k, true)) != cudaSuccess) return cuda_err(c, e, "host checkpoint copy");
-      if (k + 1 < tl.nseg && (rc = ops.advance(k * tl.L, (k + 1) * tl.L)) != MP_OK) return rc;
+      if (!skipping && (e = host_copy(k, true)) != cudaSuccess) return cuda_err(c, e, "host checkpoint copy");
+      if (k + 1 < tl.nseg && (r = ops.advance(k * tl.L, (k + 1) * tl.L)) != MP_OK) return r;
       live = k * tl.L + (k + 1 < tl.nseg ? tl.L : 0);
     }
     // segments last first, each from its host copy on the device schedule
@@ -2163,12 +2257,33 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
         c->time = t0 + a0;
         live = a0;
       }
-      if ((e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
+      if (!skipping && (e = copy_state(0, true)) != cudaSuccess) return cuda_err(c, e, "checkpoint copy");
       std::vector<int> free_slots;
       for (int q = slots - 1; q >= 1; --q) free_slots.push_back(q);
-      if ((rc = revolve(a0, a1, 0, free_slots, K, ops, live)) != MP_OK) return rc;
+      if ((r = revolve(a0, a1, 0, free_slots, K, ops, live)) != MP_OK) return r;
     }
+    return MP_OK;
+  };
+  const int rc = run_schedule();
+  if (phase == kAdjRecord) {
+    if (rc != kAdjStop) return rc == MP_OK ? set_err(c, MP_ERR_INVALID, "the run did not reach its end") : rc;
+    // the live state is the end state at time t0 + Tn; J is read
+    made->a = *a;
+    made->t0 = t0;
+    made->J = *J;
+    made->Kh = Kh;
+    made->slots = slots;
+    made->nbuf = nbuf;
+    made->two = two;
+    made->tl = tl;
+    made->ckpt = ckpt;
+    made->hist[0] = hist[0];
+    made->hist[1] = hist[1];
+    made->terms = terms;
+    c->rec = made.release();
+    return MP_OK;
   }
+  if (rc != MP_OK) return rc;
   if ((e = cudaStreamSynchronize(rs.s)) != cudaSuccess) return cuda_err(c, e, "adjoint");
   if ((e = copy_state(slots, false)) != cudaSuccess) return cuda_err(c, e, "checkpoint restore");
   c->time = t0 + Tn;
@@ -2189,13 +2304,15 @@ int mp_objective(mp_ctx *c, const mp_adjoint_config *a, double *J) {
   int rc = check_objective(c, a);
   if (rc != MP_OK) return rc;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   return c->fp32 ? objective_impl<float>(c, c->epf, c->bpf, a, J) : objective_impl<double>(c, c->epd, c->bpd, a, J);
 }
 
-int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_eps, double *grad_deps_scale,
-               double *grad_chi_scale) {
-  if (!c || !a || !J) return MP_ERR_INVALID;
-  NvtxRange nv("mp_adjoint");
+}  // extern "C"
+
+namespace {
+// What the adjoint needs of the context and the objective.
+int adjoint_supported(mp_ctx *c, const mp_adjoint_config *a) {
   int rc = check_objective(c, a);
   if (rc != MP_OK) return rc;
   if (c->mode != MODE_PLRC_LIN && c->mode != MODE_PLRC_NONLIN)
@@ -2205,14 +2322,61 @@ int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_ep
     return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint needs the xy-periodic boundary");
   if (!c->design) return set_err(c, MP_ERR_INVALID, "mp_adjoint needs a design region (mp_config.design_box)");
   if (c->tma) return set_err(c, MP_ERR_UNSUPPORTED, "mp_adjoint uses the global-load kernels");
+  return MP_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int mp_adjoint(mp_ctx *c, const mp_adjoint_config *a, double *J, double *grad_eps, double *grad_deps_scale,
+               double *grad_chi_scale) {
+  if (!c || !a || !J) return MP_ERR_INVALID;
+  NvtxRange nv("mp_adjoint");
+  int rc = adjoint_supported(c, a);
+  if (rc != MP_OK) return rc;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   double *g[3] = {grad_eps, grad_deps_scale, grad_chi_scale};
   return c->fp32 ? adjoint_impl<float>(c, c->epf, c->bpf, a, J, g) : adjoint_impl<double>(c, c->epd, c->bpd, a, J, g);
+}
+
+int mp_objective_record(mp_ctx *c, const mp_adjoint_config *a, double *J) {
+  if (!c || !a || !J) return MP_ERR_INVALID;
+  NvtxRange nv("mp_objective_record");
+  int rc = adjoint_supported(c, a);
+  if (rc != MP_OK) return rc;
+  cudaSetDevice(c->cfg.device);
+  release_record(c);
+  double *g[3] = {nullptr, nullptr, nullptr};
+  return c->fp32 ? adjoint_impl<float>(c, c->epf, c->bpf, a, J, g, kAdjRecord)
+                 : adjoint_impl<double>(c, c->epd, c->bpd, a, J, g, kAdjRecord);
+}
+
+int mp_adjoint_reverse(mp_ctx *c, double *J, double *grad_eps, double *grad_deps_scale, double *grad_chi_scale) {
+  if (!c) return MP_ERR_INVALID;
+  NvtxRange nv("mp_adjoint_reverse");
+  if (!c->rec)
+    return set_err(c, MP_ERR_INVALID,
+                   "mp_adjoint_reverse: no recorded run (mp_objective_record; calls that change the state release it)");
+  cudaSetDevice(c->cfg.device);
+  double *g[3] = {grad_eps, grad_deps_scale, grad_chi_scale};
+  const int rc = c->fp32 ? adjoint_impl<float>(c, c->epf, c->bpf, nullptr, J, g, kAdjReverse)
+                         : adjoint_impl<double>(c, c->epd, c->bpd, nullptr, J, g, kAdjReverse);
+  release_record(c);
+  return rc;
+}
+
+int mp_release_record(mp_ctx *c) {
+  if (!c) return MP_ERR_INVALID;
+  release_record(c);
+  return MP_OK;
 }
 
 int mp_set_host_checkpoint_budget(mp_ctx *c, double bytes) {
   if (!c) return MP_ERR_INVALID;
   if (!(bytes >= 0) || !std::isfinite(bytes)) return set_err(c, MP_ERR_INVALID, "host checkpoint budget %g", bytes);
+  cudaSetDevice(c->cfg.device);
+  release_record(c);
   free_host_ckpt(c);
   size_t S = 0;
   for (const auto &r : state_regions(c)) S += r.second;
@@ -2319,6 +2483,7 @@ int mp_save_state(mp_ctx *c, void *host, size_t bytes) {
 int mp_load_state(mp_ctx *c, const void *host, size_t bytes) {
   if (!c || !host) return MP_ERR_INVALID;
   cudaSetDevice(c->cfg.device);
+  release_record(c);
   const auto regions = state_regions(c);
   StateHeader want, got;
   fill_header(c, regions, want);
@@ -2369,6 +2534,7 @@ void mp_init_defaults(int kind, mp_init *q) {
 
 int mp_initialize(mp_ctx *c, const mp_init *q) {
   if (!c || !q) return MP_ERR_INVALID;
+  release_record(c);
   const mp_config &g = c->cfg;
   InitParams p;
   memset(&p, 0, sizeof p);

@@ -25,7 +25,8 @@ EXPORTED = (
     "mp_upload", "mp_download", "mp_step", "mp_step_async", "mp_check_status",
     "mp_get_time", "mp_set_time", "mp_sync", "mp_device_field", "mp_launch_count",
     "mp_last_error", "mp_create_error", "mp_kernel_times", "mp_field_energy",
-    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_set_host_checkpoint_budget", "mp_state_size", "mp_save_state",
+    "mp_field_energy_noalloc", "mp_objective", "mp_adjoint", "mp_objective_record", "mp_adjoint_reverse",
+    "mp_release_record", "mp_set_host_checkpoint_budget", "mp_state_size", "mp_save_state",
     "mp_load_state", "mp_init_defaults", "mp_initialize", "mp_follow_max", "mp_kerr_counts",
     "mp_diag_file_name", "mp_hdf5_create", "mp_hdf5_write_field", "mp_hdf5_write_slice", "mp_hdf5_write_grid", "mp_hdf5_close",
 )
@@ -90,6 +91,12 @@ def lib():
     L.mp_objective.restype = C.c_int
     L.mp_adjoint.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp, dp, dp, dp]
     L.mp_adjoint.restype = C.c_int
+    L.mp_objective_record.argtypes = [vp, C.POINTER(abi.AdjointConfig), dp]
+    L.mp_objective_record.restype = C.c_int
+    L.mp_adjoint_reverse.argtypes = [vp, dp, dp, dp, dp]
+    L.mp_adjoint_reverse.restype = C.c_int
+    L.mp_release_record.argtypes = [vp]
+    L.mp_release_record.restype = C.c_int
     L.mp_set_host_checkpoint_budget.argtypes = [vp, C.c_double]
     L.mp_set_host_checkpoint_budget.restype = C.c_int
     L.mp_state_size.argtypes = [vp, C.POINTER(sz)]
@@ -344,6 +351,30 @@ class Simulation:
         J = C.c_double()
         self._check(lib().mp_adjoint(self._h, C.byref(adj), C.byref(J), _dptr(g[0]), _dptr(g[1]), _dptr(g[2])))
         return J.value, {name: a.reshape(shape) for name, a in zip(abi.DESIGN_NAMES, g)}
+
+    def objective_record(self, adj: abi.AdjointConfig) -> float:
+        """The forward part of adjoint(adj): runs the steps, returns J and
+        keeps the checkpoints for adjoint_reverse (mp_objective_record)."""
+        J = C.c_double()
+        self._check(lib().mp_objective_record(self._h, C.byref(adj), C.byref(J)))
+        return J.value
+
+    def adjoint_reverse(self) -> tuple[float, dict]:
+        """J and the gradient of the run objective_record recorded
+        (mp_adjoint_reverse); the record is released."""
+        shape = abi.design_shape(self.cfg)
+        J = C.c_double()
+        if shape is None:
+            self._check(lib().mp_adjoint_reverse(self._h, C.byref(J), None, None, None))
+            return J.value, {}
+        n = int(np.prod(shape))
+        g = [np.empty(n) for _ in range(3)]
+        self._check(lib().mp_adjoint_reverse(self._h, C.byref(J), _dptr(g[0]), _dptr(g[1]), _dptr(g[2])))
+        return J.value, {name: a.reshape(shape) for name, a in zip(abi.DESIGN_NAMES, g)}
+
+    def release_record(self):
+        """Frees what objective_record kept (mp_release_record)."""
+        self._check(lib().mp_release_record(self._h))
 
     # -- HDF5 field dumps (FieldDiag through HDFostream)
     def write_hdf5(self, pattern: str, fields, proc_id: int = 0, time: int | None = None) -> str:

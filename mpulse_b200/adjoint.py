@@ -8,8 +8,12 @@ differentiable function of the design maps.
 
 Every evaluation starts from the problem's initial state (fields, PLRC and CPML
 state zero, time `start_time`).  When any input requires a gradient the
-forward call runs mp_adjoint (forward with checkpoints, then the discrete
-adjoint) and keeps the gradient for backward; otherwise it runs mp_objective.
+forward call runs mp_objective_record (the forward run keeping mp_adjoint's
+checkpoints) and backward runs mp_adjoint_reverse (the reverse pass) on the
+same simulation; otherwise forward runs mp_objective.  If another evaluation
+of the problem has replaced the simulation before backward, backward runs
+mp_adjoint from the initial state with the maps of its own forward call (the
+same gradient).
 The maps travel as FP64 host arrays through the C ABI; the result has the
 dtype and device of the first map.
 """
@@ -60,19 +64,30 @@ class DesignObjective(torch.autograd.Function):
                 maps[name] = t.detach().to("cpu", torch.float64).numpy().reshape(shape)
         sim = problem.reset(maps)
         ref = eps if eps is not None else (dscale if dscale is not None else chiscale)
+        ctx.problem, ctx.maps, ctx.sim = problem, maps, sim
+        ctx.device, ctx.dtype = ref.device, ref.dtype
         if any(ctx.needs_input_grad[1:]):
-            J, grads = sim.adjoint(problem.adj)
-            ctx.grads = [torch.from_numpy(grads[n]).to(ref.device, ref.dtype) for n in abi.DESIGN_NAMES]
+            J = sim.objective_record(problem.adj)
         else:
             J = sim.objective(problem.adj)
-            ctx.grads = None
         return torch.tensor(J, dtype=ref.dtype, device=ref.device)
 
     @staticmethod
     def backward(ctx, gJ):
+        problem = ctx.problem
+        grads = None
+        if problem.sim is ctx.sim:
+            try:
+                _, grads = ctx.sim.adjoint_reverse()
+            except runtime.MPulseError:
+                grads = None  # the record was released: run the whole adjoint below
+        if grads is None:
+            _, grads = problem.reset(ctx.maps).adjoint(problem.adj)
+        ctx.sim = None
         out = [None]
-        for k in range(3):
-            out.append(gJ * ctx.grads[k] if ctx.needs_input_grad[1 + k] else None)
+        for k, name in enumerate(abi.DESIGN_NAMES):
+            g = torch.from_numpy(grads[name]).to(ctx.device, ctx.dtype)
+            out.append(gJ * g if ctx.needs_input_grad[1 + k] else None)
         return tuple(out)
 
 

@@ -115,8 +115,9 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // the design gradients are FP64.  One thread per (x, y) column marches up a
 // chunk of planes, carrying the z-neighbours in registers.  Arrays a kernel
 // only reads (the B adjoint in adj_e, G in adj_b, the E history) go through
-// the read-only data path (ldg_c).
-template <typename T, int NP>
+// the read-only data path (ldg_c).  NL: the Kerr medium (PLRC nonlinear); the
+// linear form leaves out the Kerr linearisation, whose terms are zero there.
+template <typename T, int NP, bool NL>
 __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_MIN_F : MPB_ADJ_E_MIN_D) / MPB_ADJ_THREADS)
     adj_e_kernel(const AdjParams<T> p) {
   typedef T R;
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
   R bx_km = ldg_c(Bx, (long long)(k0 - 1) * pl + col, nf, st);
   R by_km = ldg_c(By, (long long)(k0 - 1) * pl + col, nf, st);
 
-  const bool plrc_nl = p.nonlin != 0;
+  const bool plrc_nl = NL;
   for (int k = k0; k <= k1; ++k) {
     const long long base = (long long)k * pl;
     const long long c0 = base + col;
@@ -276,17 +277,17 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
         ne[c] = p.eps_bg_t * g[c];
       }
     } else {
-      double A = p.A0;
-      R idn = p.inv_denom0_t, numer = p.numer0_t, Rchi = p.chi_nl_t;
+      double A = NL ? p.A0 : 0.0;
+      R idn = p.inv_denom0_t, numer = p.numer0_t, Rchi = NL ? p.chi_nl_t : R(0);
       if (dcell) {
         const double denom = d.lin ? e + s * (p.sumChi0 - p.sumXi0) : e + s * p.sumChi0 - s * p.sumXi0;
-        A = p.nonlin ? u * p.chi / denom : 0.0;
+        A = NL ? u * p.chi / denom : 0.0;
         idn = R(1.0 / denom);
         numer = R(e - s * p.sumXi0);
-        Rchi = R(p.nonlin ? u * p.chi : 0.0);
+        Rchi = NL ? R(u * p.chi) : R(0);
       }
       R cb[3] = {a[0], a[1], a[2]};
-      if (plrc_nl) {
+      if (NL) {
         // E' = r c/|c| with r + A r^3 = |c|: dE'/dc = (I - e e^T) / (1 + A r^2)
         // + e e^T / (1 + 3 A r^2), dr/dA = -r^3 / (1 + 3 A r^2), c = E' (1 + A r^2)
         const double r2 = (double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2];
@@ -302,13 +303,18 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
 #pragma unroll
         for (int c = 0; c < 3; ++c) cb[c] = R(al * (a[c] - eh[c] * ea) + be * eh[c] * ea);
       }
-      const R E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
 #pragma unroll
       for (int c = 0; c < 3; ++c) g[c] = cb[c] * idn;
-      const R Eg = En[0] * g[0] + En[1] * g[1] + En[2] * g[2];
-      const R f = numer + Rchi * E2;
+      if (NL) {
+        const R E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
+        const R Eg = En[0] * g[0] + En[1] * g[1] + En[2] * g[2];
+        const R f = numer + Rchi * E2;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) ne[c] = f * g[c] + R(2) * Rchi * En[c] * Eg;
+        for (int c = 0; c < 3; ++c) ne[c] = f * g[c] + R(2) * Rchi * En[c] * Eg;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ne[c] = numer * g[c];
+      }
       // the design cells' accumulator adjoints before the reverse recursion,
       // for adj_grad
       if (dcell) {
@@ -403,7 +409,7 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_E_M
 // the adjoint of A through the Kerr solve, is -(e^ . c_bar) r^3 with r = |E'|,
 // e^ = E' / r and c_bar = g denom the adjoint of c (the Kerr linearisation of
 // adj_e gives e^ . c_bar = be (e^ . a) with be = 1 / (1 + 3 A r^2)).
-template <typename T, int NP>
+template <typename T, int NP, bool NL>
 __device__ __forceinline__ void adj_grad_cells(const AdjParams<T> &p, int gbx, int gby, int kk) {
   const DesignParams &d = p.design;
   const int ii = gbx * blockDim.x + threadIdx.x, jj = gby * blockDim.y + threadIdx.y;
@@ -425,17 +431,16 @@ __device__ __forceinline__ void adj_grad_cells(const AdjParams<T> &p, int gbx, i
   }
   const double dD = p.sumChi0 - p.sumXi0;
   const double denom = d.lin ? e + s * dD : e + s * p.sumChi0 - s * p.sumXi0;
-  const double A = p.nonlin ? u * p.chi / denom : 0.0;
-  const double r2 = (double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2];
+  const double A = NL ? u * p.chi / denom : 0.0;
+  const double r2 = NL ? (double)En1[0] * En1[0] + (double)En1[1] * En1[1] + (double)En1[2] * En1[2] : 0.0;
   double Abar = 0.0;
-  if (p.nonlin && r2 > 0) {
+  if (NL && r2 > 0) {
     const double r = sqrt(r2);
     double ecb = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) ecb += (double)En1[c] / r * ((double)g[c] * denom);
     Abar = -ecb * r * r2;
   }
-  const T E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
   double gs = 0.0, SD = 0.0;
 #pragma unroll
   for (int n = 0; n < NP; ++n) {
@@ -449,16 +454,17 @@ __device__ __forceinline__ void adj_grad_cells(const AdjParams<T> &p, int gbx, i
       gs += (pr * (p.pxi[n][0] + CDr) + pim * (p.pxi[n][1] + CDi)) * (double)En[c];
     }
   }
-  double ge = -Abar * A / denom, gu = 0.0;
-  gs -= Abar * A * dD / denom;
-  const double grow = 1.0 + A * r2;
+  double ge = NL ? -Abar * A / denom : 0.0, gu = 0.0;
+  if (NL) gs -= Abar * A * dD / denom;
+  const double grow = NL ? 1.0 + A * r2 : 1.0;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const double cv = (double)En1[c] * grow;
     ge += (double)g[c] * ((double)En[c] - cv);
     gs += (double)g[c] * ((SD - p.sumXi0) * (double)En[c] - cv * dD);
   }
-  if (p.nonlin) {
+  if (NL) {
+    const T E2 = En[0] * En[0] + En[1] * En[1] + En[2] * En[2];
     gu = Abar * p.chi / denom;
 #pragma unroll
     for (int c = 0; c < 3; ++c) gu += (double)g[c] * p.chi * (double)E2 * (double)En[c];
@@ -615,7 +621,7 @@ __device__ __forceinline__ void adj_b_cells(const AdjParams<T> &p, int bxi, int 
 // x fastest over gx x gy x z-chunks) and the design gradients of the step
 // (the blocks after them, over the design box in 32 x 4 tiles, one plane
 // each).
-template <typename T, int NP>
+template <typename T, int NP, bool NL>
 __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_MIN_F : MPB_ADJ_B_MIN_D) / MPB_ADJ_THREADS)
     adj_b_kernel(const AdjParams<T> p, const int gx, const int gy, const int nb) {
   pdl_launch_dependents();
@@ -625,7 +631,7 @@ __global__ void __launch_bounds__(MPB_ADJ_THREADS, (sizeof(T) == 4 ? MPB_ADJ_B_M
   } else {
     const int q = b - nb;
     const int tx = (p.design.bx + 31) / 32, ty = (p.design.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y;
-    adj_grad_cells<T, NP>(p, q % tx, (q / tx) % ty, q / (tx * ty));
+    adj_grad_cells<T, NP, NL>(p, q % tx, (q / tx) % ty, q / (tx * ty));
   }
 }
 
@@ -745,11 +751,12 @@ template <typename T>
 cudaError_t launch_adj_e(const AdjParams<T> &p, cudaStream_t st) {
   const dim3 b(32, MPB_ADJ_BLOCK_Y, 1),
       g((p.nx + 31) / 32, (p.ny + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y, (p.nz + p.kchunk_e - 1) / p.kchunk_e);
+  const bool nl = p.nonlin != 0;
   switch (p.np) {
-    case 0: return launch_pdl(adj_e_kernel<T, 0>, g, b, st, p);
-    case 1: return launch_pdl(adj_e_kernel<T, 1>, g, b, st, p);
-    case 2: return launch_pdl(adj_e_kernel<T, 2>, g, b, st, p);
-    default: return launch_pdl(adj_e_kernel<T, 3>, g, b, st, p);
+    case 0: return nl ? launch_pdl(adj_e_kernel<T, 0, true>, g, b, st, p) : launch_pdl(adj_e_kernel<T, 0, false>, g, b, st, p);
+    case 1: return nl ? launch_pdl(adj_e_kernel<T, 1, true>, g, b, st, p) : launch_pdl(adj_e_kernel<T, 1, false>, g, b, st, p);
+    case 2: return nl ? launch_pdl(adj_e_kernel<T, 2, true>, g, b, st, p) : launch_pdl(adj_e_kernel<T, 2, false>, g, b, st, p);
+    default: return nl ? launch_pdl(adj_e_kernel<T, 3, true>, g, b, st, p) : launch_pdl(adj_e_kernel<T, 3, false>, g, b, st, p);
   }
 }
 
@@ -764,11 +771,12 @@ cudaError_t launch_adj_b(const AdjParams<T> &p, cudaStream_t st) {
   const int ng = d.x0 <= d.x1 ? ((d.bx + 31) / 32) * ((d.by + MPB_ADJ_BLOCK_Y - 1) / MPB_ADJ_BLOCK_Y) * (d.z1 - d.z0 + 1)
                               : 0;
   const dim3 b(32, MPB_ADJ_BLOCK_Y, 1), g(nb + ng, 1, 1);
+  const bool nl = p.nonlin != 0;
   switch (p.np) {
-    case 0: return launch_pdl(adj_b_kernel<T, 0>, g, b, st, p, gx, gy, nb);
-    case 1: return launch_pdl(adj_b_kernel<T, 1>, g, b, st, p, gx, gy, nb);
-    case 2: return launch_pdl(adj_b_kernel<T, 2>, g, b, st, p, gx, gy, nb);
-    default: return launch_pdl(adj_b_kernel<T, 3>, g, b, st, p, gx, gy, nb);
+    case 0: return nl ? launch_pdl(adj_b_kernel<T, 0, true>, g, b, st, p, gx, gy, nb) : launch_pdl(adj_b_kernel<T, 0, false>, g, b, st, p, gx, gy, nb);
+    case 1: return nl ? launch_pdl(adj_b_kernel<T, 1, true>, g, b, st, p, gx, gy, nb) : launch_pdl(adj_b_kernel<T, 1, false>, g, b, st, p, gx, gy, nb);
+    case 2: return nl ? launch_pdl(adj_b_kernel<T, 2, true>, g, b, st, p, gx, gy, nb) : launch_pdl(adj_b_kernel<T, 2, false>, g, b, st, p, gx, gy, nb);
+    default: return nl ? launch_pdl(adj_b_kernel<T, 3, true>, g, b, st, p, gx, gy, nb) : launch_pdl(adj_b_kernel<T, 3, false>, g, b, st, p, gx, gy, nb);
   }
 }
 

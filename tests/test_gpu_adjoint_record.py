@@ -135,3 +135,28 @@ def test_reads_keep_the_record():
     assert J1 == J0
     for name in abi.DESIGN_NAMES:
         assert np.array_equal(g1[name], g0[name]), name
+
+
+def test_autograd_backward_after_another_evaluation():
+    """Two evaluations of one problem before backward: the first one's record
+    was released by the second, so its backward runs mp_adjoint from the
+    initial state; both gradients equal mp_adjoint's."""
+    import torch
+    from mpulse_b200 import adjoint
+
+    cfg = design_case(abi.MP_SOLVER_PLRC_NONLIN, abi.MP_CPML_Z, source=True)
+    des = design_maps(cfg, 39)
+    init = clean_init(cfg, 40, smooth=True, scale=0.2)
+    adj = abi.adjoint_config(abi.MP_OBJ_E2_BOX, BOXES[abi.MP_OBJ_E2_BOX], 14, checkpoint_every=5)
+    problem = adjoint.DesignProblem(cfg, init, adj)
+    eps1 = torch.tensor(des["DesignEps"], dtype=torch.float64, requires_grad=True)
+    eps2 = torch.tensor(des["DesignEps"] * 1.01, dtype=torch.float64, requires_grad=True)
+    J1 = adjoint.design_objective(problem, eps1)
+    J2 = adjoint.design_objective(problem, eps2)
+    (J1 + J2).backward()
+    problem.close()
+    for eps, t in ((eps1, des["DesignEps"]), (eps2, des["DesignEps"] * 1.01)):
+        # the other maps keep their defaults, as in the evaluations above
+        with gpu_sim(cfg, init, {"DesignEps": t}) as g:
+            _, ref = g.adjoint(adj)
+        assert np.array_equal(eps.grad.numpy(), ref["DesignEps"])

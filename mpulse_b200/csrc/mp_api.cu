@@ -2115,6 +2115,14 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   auto hist_into = [&](long long slot) {
     for (int q = 0; q < 3; ++q) ep.hist[q] = slot < 0 ? nullptr : const_cast<T *>(slot_e(slot, q));
   };
+  // The E kernel stores the history where the reverse kernels read it: every
+  // cell for the Kerr linearisation, otherwise the design cells (adj_e's E^{n+1}
+  // and the gradients) and the objective's box or plane; the other cells of a
+  // slot are never read.  (Slot 0 of a chunk is a copy of the whole E.)
+  ep.hist_all = p.nonlin;
+  const int hb[2][6] = {{c->dp.x0, c->dp.x1, c->dp.y0, c->dp.y1, c->dp.z0, c->dp.z1},
+                        {b0[0], b0[1], b0[2], b0[3], b0[4], b0[5]}};
+  memcpy(ep.hist_box, hb, sizeof hb);
   // ---- forward and reverse on the checkpoint schedule
   const long long t0 = rec ? rec->t0 : c->time;
   long long reached = 0;  // steps whose objective term is computed

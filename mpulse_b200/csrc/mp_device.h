@@ -114,6 +114,10 @@ struct EParams {
   CpmlFace<T> cpml[6];    // E-side CPML currents in MPulse's current order
   DesignParams design;
   T *hist[3];             // with a design region: also store the new E here (adjoint history), if set
+  // the cells whose history the reverse pass reads: all (hist_all) or those in
+  // either box (0-based x0, x1, y0, y1, MPulse z0, z1; x0 > x1: empty)
+  int hist_all;
+  int hist_box[2][6];
   int n_src;
   int src_mult;           // how many injectors share the plane (each adds it once)
   SourcePlane<T> src[4];

@@ -109,6 +109,18 @@
 
 namespace mpb {
 
+// Whether the adjoint history of cell (i, j, k) is stored (EParams::hist_box).
+template <typename T>
+__device__ __forceinline__ bool hist_cell(const EParams<T> &p, int i, int j, int k) {
+  if (p.hist_all) return true;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const int *h = p.hist_box[b];
+    if (i >= h[0] && i <= h[1] && j >= h[2] && j <= h[3] && k >= h[4] && k <= h[5]) return true;
+  }
+  return false;
+}
+
 template <typename T, int MODE, int NP, bool DESIGN, bool PLASMA = false>
 __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y,
                                   (sizeof(T) == 4 ? MPB_E_MIN_THREADS_F : MPB_E_MIN_THREADS) / (32 * MPB_E_BLOCK_Y))
@@ -205,7 +217,7 @@ __global__ void __launch_bounds__(32 * MPB_E_BLOCK_Y,
         st_c(p.pj[2], base + col, nf, st, pc.j[2]);
       }
     }
-    if (DESIGN && p.hist[0]) {
+    if (DESIGN && p.hist[0] && hist_cell(p, i, j, k)) {
       st_c(p.hist[0], base + col, nf, st, exn);
       st_c(p.hist[1], base + col, nf, st, eyn);
       st_c(p.hist[2], base + col, nf, st, ezn);

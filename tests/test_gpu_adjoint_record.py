@@ -67,6 +67,30 @@ def test_record_and_reverse_equal_adjoint(schedule, precision):
     assert np.any(g1["DesignEps"])
 
 
+@pytest.mark.parametrize("every,host_states", [(7, 0), (0, 12)], ids=["every_7", "two_level"])
+def test_record_and_reverse_sz_plane(every, host_states):
+    """The Sz-plane objective, whose history also keeps Bx and By on the plane,
+    in a linear medium (E history stored only at the design cells and on the
+    plane)."""
+    cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_ALL, source=True)
+    des = design_maps(cfg, 41)
+    init = clean_init(cfg, 42, smooth=True, scale=0.2)
+    box = BOXES[abi.MP_OBJ_SZ_PLANE]
+    if every:
+        adj = abi.adjoint_config(abi.MP_OBJ_SZ_PLANE, box, STEPS, checkpoint_every=every)
+    else:
+        adj = abi.adjoint_config(abi.MP_OBJ_SZ_PLANE, box, STEPS, mem_budget=516.0 * cfg.field_count())
+    with setup(cfg, init, des, host_states) as g:
+        J0, g0 = g.adjoint(adj)
+    with setup(cfg, init, des, host_states) as g:
+        Jr = g.objective_record(adj)
+        J1, g1 = g.adjoint_reverse()
+    assert Jr == J0 == J1
+    for name in abi.DESIGN_NAMES:
+        assert np.array_equal(g1[name], g0[name]), name
+    assert np.any(g1["DesignEps"])
+
+
 def test_reverse_twice_and_without_record():
     cfg = design_case(abi.MP_SOLVER_PLRC_LIN, abi.MP_CPML_Z, source=True)
     des = design_maps(cfg, 33)

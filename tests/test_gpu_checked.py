@@ -1,5 +1,5 @@
 """The bounds-checked build (libmpulse_b200_checked.so, MPB_CHECKED=1) on
-every forward parity case, every adjoint case and the fused step form's
+every forward parity case, every adjoint case (one call and two) and the fused step form's
 cases: its step, fused-step, border and adjoint
 kernels test each field, history, PLRC, CPML, design and injection-plane
 index against the size of its array and make mp_step / mp_adjoint fail with
@@ -21,7 +21,8 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.mark.parametrize("suite", ["test_gpu_parity.py", "test_gpu_adjoint.py", "test_gpu_fused.py"])
+@pytest.mark.parametrize("suite", ["test_gpu_parity.py", "test_gpu_adjoint.py", "test_gpu_adjoint_record.py",
+                                   "test_gpu_fused.py"])
 def test_suite_passes_through_the_checked_build(suite):
     assert os.path.exists(build.LIB_CHECKED), "build the checked library: python -m mpulse_b200.build --checked"
     env = dict(os.environ, MPULSE_B200_LIB=build.LIB_CHECKED)

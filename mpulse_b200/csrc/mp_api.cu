@@ -2128,6 +2128,12 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   long long reached = 0;  // steps whose objective term is computed
   bool at_end = false;
   bool skipping = rec != nullptr;  // replaying what the recorded run did
+  // With a checkpoint at every chunk start and two history buffers, the first
+  // run also keeps the history of the chunk before the last, [prev0, last0),
+  // in buffer 1: that chunk is then reversed without being run again.
+  const bool keep2 = nbuf == 2 && a->checkpoint_every > 0 && !two;
+  const long long last0 = ((Tn - 1) / K) * K, prev0 = last0 - K;
+  bool prev_kept = false;  // its history is in buffer 1 and not yet reversed
   // Forward steps n0..n1-1 from the live state in one batched call: the E
   // kernel of step n stores the new E into history slot n + 1 - h0 when
   // n >= h0 (h0 < 0: no history), the Sz planes are copied after it, and the
@@ -2154,7 +2160,7 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
   };
   RevolveOps ops;
   ops.restore = [&](long long at, int slot) -> int {
-    if (skipping) return MP_OK;
+    if (skipping || (prev_kept && at == prev0)) return MP_OK;
     const cudaError_t err = copy_state(slot, false);
     c->time = t0 + at;
     return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint restore");
@@ -2165,18 +2171,34 @@ int adjoint_impl(mp_ctx *c, EParams<T> &ep, BParams<T> &bp, const mp_adjoint_con
     return err == cudaSuccess ? MP_OK : cuda_err(c, err, "checkpoint copy");
   };
   ops.advance = [&](long long from, long long to) -> int {
+    // the first run's advance to the last chunk runs the chunk before it
+    // into history buffer 1
+    const bool split = keep2 && !at_end && to == last0 && from <= prev0;
+    if (split) prev_kept = true;
     if (skipping) {
       reached = std::max(reached, to);
       return MP_OK;
     }
     NvtxRange nv("mp_adjoint forward");
-    return run(from, to, -1);
+    const long long mid = split ? prev0 : to;
+    int r = mid > from ? run(from, mid, -1) : MP_OK;
+    if (r != MP_OK || !split) return r;
+    cur = 1;
+    const cudaError_t err = record(0, true);
+    r = err == cudaSuccess ? run(prev0, to, prev0) : cuda_err(c, err, "history copy");
+    cur = 0;
+    return r;
   };
   ops.leaf = [&](long long n0, long long n1) -> int {
     NvtxRange nv("mp_adjoint chunk");
     cudaError_t err;
     const bool first = n1 == Tn && !at_end;
-    if (skipping) {
+    if (prev_kept && n0 == prev0) {
+      // its history is in buffer 1 from the first run (the buffer the last
+      // chunk's reverse pass left next)
+      if (cur != 1 || rs.used[1]) return set_err(c, MP_ERR_INVALID, "kept history out of order");
+      prev_kept = false;
+    } else if (skipping) {
       // the recorded run ended with this chunk's forward run: its history is
       // in buffer 0, J and the final state are kept
       if (!first || cur != 0) return set_err(c, MP_ERR_INVALID, "recorded schedule does not replay");

@@ -79,10 +79,12 @@ def test_objective_matches_oracle(kind):
 
 @pytest.mark.parametrize("solver", [abi.MP_SOLVER_PLRC_LIN, abi.MP_SOLVER_PLRC_NONLIN])
 @pytest.mark.parametrize("kind", [abi.MP_OBJ_E2_BOX, abi.MP_OBJ_SZ_PLANE])
-@pytest.mark.parametrize("every", [0, 5])
+@pytest.mark.parametrize("every", [0, 5, 8])
 def test_fp64_adjoint_matches_restatement(solver, kind, every):
     """checkpoint_every 0 keeps the whole history from the forward run; 5
-    recomputes the segments [0,5), [5,10) from checkpoints."""
+    recomputes the segment [0,5) from its checkpoint ([5,10) keeps its history
+    from the first run); 8 has two segments, the first kept from the first
+    run."""
     cfg = design_case(solver, abi.MP_CPML_ALL, source=True)
     des = design_maps(cfg, 16)
     init = clean_init(cfg, 17, smooth=True, scale=0.2)

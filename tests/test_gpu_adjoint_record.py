@@ -24,6 +24,7 @@ def schedules(cfg):
     return {
         "whole_history": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS), 0),
         "every_7": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS, checkpoint_every=7), 0),
+        "every_20": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS, checkpoint_every=20), 0),
         "every_30": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS, checkpoint_every=30), 0),
         "budget_3_slots": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS, mem_budget=648.0 * n), 0),
         "budget_1_slot": (abi.adjoint_config(abi.MP_OBJ_E2_BOX, box, STEPS, mem_budget=516.0 * n), 0),
@@ -39,8 +40,8 @@ def setup(cfg, init, des, host_states):
 
 
 @pytest.mark.parametrize("precision", [abi.MP_FP64, abi.MP_FP32], ids=["fp64", "fp32"])
-@pytest.mark.parametrize("schedule", ["whole_history", "every_7", "every_30", "budget_3_slots", "budget_1_slot",
-                                      "two_level"])
+@pytest.mark.parametrize("schedule", ["whole_history", "every_7", "every_20", "every_30", "budget_3_slots",
+                                      "budget_1_slot", "two_level"])
 def test_record_and_reverse_equal_adjoint(schedule, precision):
     cfg = design_case(abi.MP_SOLVER_PLRC_NONLIN, abi.MP_CPML_Z, source=True)
     cfg.precision = precision

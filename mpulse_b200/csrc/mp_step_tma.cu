@@ -16,7 +16,7 @@
 // memory.  x halos start 16 bytes before / at the tile (the TMA x coordinate
 // must be a multiple of 16 bytes); a halo that falls outside the grid reads as
 // zero and the few cells that need the periodic image read it from global
-// memory instead.  No cluster, no multicast.
+// memory instead.  Each CTA loads its own tiles; no thread-block clusters.
 //
 // Every wait on an mbarrier is bounded: after ~4M polls the warp records a
 // timeout in the status word and leaves; mp_step then reports MP_ERR_CUDA.
